@@ -1,0 +1,353 @@
+"""Python mirror of the reference's forward-solve entry points over the C ABI.
+
+Method names follow ``src/em_fwd.h`` and ``src/em_la.h`` of the reference
+(create_linear_system, assemble_matrix, create_pc, solve_linear_system,
+estimate_error, ...); errors surface as :class:`EMGError` carrying the C-ABI
+status (``EMG_ERR_USER`` = the reference's ``EM_ERR_USER`` = -1).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+EMG_OK = 0
+EMG_ERR_USER = -1
+EMG_ERR_ARG = -2
+EMG_ERR_STATE = -3
+EMG_ERR_CUDA = -4
+EMG_ERR_NOMEM = -5
+EMG_DIVERGED_ITS = -6
+EMG_DIVERGED_NANORINF = -7
+EMG_ERR_OPTION = -8
+
+XY_POLAR, YX_POLAR = -1, -2      # src/em_defs.h:39
+SOL_CSEM, SOL_DUAL = 0, 1
+
+
+class EMGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("emfem_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("outer_its", C.c_int), ("inner_its", C.c_int), ("reason", C.c_int),
+                ("true_rel_res", C.c_double), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BlockOpts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("max_it", C.c_int), ("use_guess", C.c_int),
+                ("inner_fp32", C.c_int), ("restart", C.c_int)]
+
+
+def library_path() -> str:
+    return os.path.join(_HERE, "libemfem_b200.so")
+
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_SIGS = {
+    "emg_last_error": ([], C.c_char_p),
+    "emg_version": ([], C.c_char_p),
+    "emg_create_context": ([C.POINTER(_P), _I], _I),
+    "emg_destroy_context": ([_P], _I),
+    "emg_process_options": ([_P, C.c_char_p], _I),
+    "emg_get_option": ([_P, C.c_char_p, C.POINTER(_D)], _I),
+    "emg_set_mesh": ([_P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P], _I),
+    "emg_set_model": ([_P, _I, _I, _I, _P], _I),
+    "emg_set_frequencies": ([_P, _I, _P], _I),
+    "emg_create_linear_system": ([_P, _I], _I),
+    "emg_destroy_linear_system": ([_P], _I),
+    "emg_get_sparsity": ([_P, C.POINTER(C.c_long), _P, _P], _I),
+    "emg_assemble_matrix": ([_P, _I], _I),
+    "emg_get_matrices": ([_P, _P, _P, _P], _I),
+    "emg_create_pc": ([_P], _I),
+    "emg_destroy_pc": ([_P], _I),
+    "emg_matshell_mult_a": ([_P, _P, _P], _I),
+    "emg_pc_apply_b": ([_P, _P, _P], _I),
+    "emg_solve_linear_system": ([_P, _I, _P, _P, _I, _D, C.POINTER(SolveInfo)], _I),
+    "emg_get_solution": ([_P, _I, _P, _P], _I),
+    "emg_set_solution": ([_P, _I, _P, _P], _I),
+    "emg_set_background": ([_P, _P, _P, _P, _P, _I], _I),
+    "emg_assemble_rhs_mt": ([_P, _I, _I, _P, _P], _I),
+    "emg_assemble_rhs_csem": ([_P, _I, _P, _P, _P, _P], _I),
+    "emg_assemble_rhs_dual": ([_P, _I, _P, _P, _P, _P], _I),
+    "emg_estimate_error": ([_P, _I, _I, _P, _P], _I),
+    "emg_refine_fixed_fraction": ([_I, _P, _D, _P], _I),
+    "emg_refine_fixed_number": ([_I, _P, _D, _P], _I),
+    "emg_interpolate_fields": ([_P, _I, _I, _I, _P, _P, _P], _I),
+    "emg_solve_block": ([_P, _I, _P, _P, _P, C.POINTER(BlockOpts), _P], _I),
+    "emg_solve_block_dev": ([_P, _I, _P, _P, _P, C.POINTER(BlockOpts), _P], _I),
+    "emg_spmv_complex_dev": ([_P, _I, _P, _P, _P, _I], _I),
+    "emg_last_kernel_ms": ([_P, C.c_char_p, C.POINTER(_D)], _I),
+    "emg_stream_synchronize": ([_P], _I),
+}
+
+
+def lib():
+    """Loads libemfem_b200.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise EMGError(EMG_ERR_STATE, "%s is not built (run __graft_entry__.build())" % path)
+        L = C.CDLL(path)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _LIB = L
+    return _LIB
+
+
+def _check(rc):
+    if rc != EMG_OK:
+        raise EMGError(rc, lib().emg_last_error().decode())
+    return rc
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def refine_fixed_fraction(err, fraction, flag=None):
+    """refine_fixed_fraction (src/em_fwd.cc:1182-1215); ORs into flag."""
+    err = _f64(err)
+    flag = np.zeros(err.size, dtype=np.uint8) if flag is None else flag
+    _check(lib().emg_refine_fixed_fraction(err.size, _ptr(err), float(fraction), _ptr(flag)))
+    return flag
+
+
+def refine_fixed_number(err, fraction, flag=None):
+    """refine_fixed_number (src/em_fwd.cc:1217-1240); ORs into flag."""
+    err = _f64(err)
+    flag = np.zeros(err.size, dtype=np.uint8) if flag is None else flag
+    _check(lib().emg_refine_fixed_number(err.size, _ptr(err), float(fraction), _ptr(flag)))
+    return flag
+
+
+class EMContext:
+    """Device-resident counterpart of the reference's EMContext (src/em_ctx.h:15-64).
+
+    ``device=-1`` gives a host-only context (options and host helpers only)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().emg_create_context(C.byref(h), int(device)))
+        self._h = h
+        self.device = device
+        self.ne = self.nt = self.nv = 0
+        self.freqs = np.zeros(0)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().emg_destroy_context(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- configuration ---------------------------------------------------------------
+    def process_options(self, text: str):
+        _check(lib().emg_process_options(self._h, text.encode()))
+
+    def get_option(self, key: str) -> float:
+        v = C.c_double()
+        _check(lib().emg_get_option(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def set_mesh(self, m):
+        self._mesh = m
+        arrs = dict(pts=_f64(m.points), tets=_i32(m.tets), attr=_i32(m.attr), edges=_i32(m.edges),
+                    t2e=_i32(m.tet2edge), nbr=_i32(m.neighbors), non=_i32(m.tet_non),
+                    ebdr=np.ascontiguousarray(m.edge_bdr, dtype=np.uint8))
+        _check(lib().emg_set_mesh(self._h, m.n_vertices, _ptr(arrs["pts"]), m.n_tets, _ptr(arrs["tets"]),
+                                  _ptr(arrs["attr"]), m.n_edges, _ptr(arrs["edges"]), _ptr(arrs["t2e"]),
+                                  _ptr(arrs["nbr"]), _ptr(arrs["non"]), _ptr(arrs["ebdr"])))
+        self.nv, self.nt, self.ne = m.n_vertices, m.n_tets, m.n_edges
+
+    def set_model(self, model):
+        rho = _f64(model.rho)
+        _check(lib().emg_set_model(self._h, int(model.aniso_form), rho.shape[0], rho.shape[1], _ptr(rho)))
+
+    def set_frequencies(self, freqs):
+        self.freqs = _f64(freqs)
+        _check(lib().emg_set_frequencies(self._h, self.freqs.size, _ptr(self.freqs)))
+
+    # -- em_fwd.h / em_la.h ---------------------------------------------------------------
+    def create_linear_system(self, tidx: int):
+        _check(lib().emg_create_linear_system(self._h, int(tidx)))
+
+    def destroy_linear_system(self):
+        _check(lib().emg_destroy_linear_system(self._h))
+
+    def make_sparsity_patterns(self):
+        nnz = C.c_long()
+        _check(lib().emg_get_sparsity(self._h, C.byref(nnz), None, None))
+        rp = np.zeros(self.ne + 1, dtype=np.int32)
+        ci = np.zeros(nnz.value, dtype=np.int32)
+        _check(lib().emg_get_sparsity(self._h, C.byref(nnz), _ptr(rp), _ptr(ci)))
+        return rp, ci
+
+    def assemble_matrix(self, fidx: int):
+        _check(lib().emg_assemble_matrix(self._h, int(fidx)))
+
+    def get_matrices(self):
+        nnz = C.c_long()
+        _check(lib().emg_get_sparsity(self._h, C.byref(nnz), None, None))
+        Cv = np.zeros(nnz.value)
+        Mv = np.zeros(nnz.value)
+        bdr = np.zeros(self.nt, dtype=np.uint8)
+        _check(lib().emg_get_matrices(self._h, _ptr(Cv), _ptr(Mv), _ptr(bdr)))
+        return Cv, Mv, bdr
+
+    def create_pc(self):
+        _check(lib().emg_create_pc(self._h))
+
+    def destroy_pc(self):
+        _check(lib().emg_destroy_pc(self._h))
+
+    def matshell_mult_a(self, x):
+        x = _f64(x)
+        y = np.zeros(2 * self.ne)
+        _check(lib().emg_matshell_mult_a(self._h, _ptr(x), _ptr(y)))
+        return y
+
+    def pc_apply_b(self, b):
+        b = _f64(b)
+        x = np.zeros(2 * self.ne)
+        _check(lib().emg_pc_apply_b(self._h, _ptr(b), _ptr(x)))
+        return x
+
+    def solve_linear_system(self, target, s_re, s_im, max_it=100, rtol=1e-8, raise_on_diverge=True):
+        info = SolveInfo()
+        rc = lib().emg_solve_linear_system(self._h, int(target), _ptr(_f64(s_re)), _ptr(_f64(s_im)), int(max_it),
+                                           float(rtol), C.byref(info))
+        if rc != EMG_OK and (raise_on_diverge or rc != EMG_DIVERGED_ITS):
+            _check(rc)
+        return info
+
+    def get_solution(self, target):
+        re = np.zeros(self.ne)
+        im = np.zeros(self.ne)
+        _check(lib().emg_get_solution(self._h, int(target), _ptr(re), _ptr(im)))
+        return re, im
+
+    def set_solution(self, target, re, im):
+        _check(lib().emg_set_solution(self._h, int(target), _ptr(_f64(re)), _ptr(_f64(im))))
+
+    def set_background(self, corners, nlay, ztop, lsig, maxl=None):
+        """Layered columns under the four top corners (update_background_model);
+        ztop/lsig are (4, maxl)."""
+        ztop = _f64(ztop).reshape(4, -1)
+        lsig = _f64(lsig).reshape(4, -1)
+        maxl = ztop.shape[1] if maxl is None else int(maxl)
+        _check(lib().emg_set_background(self._h, _ptr(_f64(corners)), _ptr(_i32(nlay)), _ptr(ztop),
+                                        _ptr(lsig), maxl))
+
+    def assemble_rhs_mt(self, fidx, mode):
+        sr = np.zeros(self.ne)
+        si = np.zeros(self.ne)
+        _check(lib().emg_assemble_rhs_mt(self._h, int(fidx), int(mode), _ptr(sr), _ptr(si)))
+        return sr, si
+
+    def assemble_rhs_csem(self, fidx, tx, dipole_tets):
+        sr = np.zeros(self.ne)
+        si = np.zeros(self.ne)
+        _check(lib().emg_assemble_rhs_csem(self._h, int(fidx), _ptr(_f64(tx)), _ptr(_i32(dipole_tets)),
+                                           _ptr(sr), _ptr(si)))
+        return sr, si
+
+    def assemble_rhs_dual(self, rx, rx_tets):
+        rx = _f64(rx).reshape(-1, 3)
+        sr = np.zeros(self.ne)
+        si = np.zeros(self.ne)
+        _check(lib().emg_assemble_rhs_dual(self._h, rx.shape[0], _ptr(rx), _ptr(_i32(rx_tets)), _ptr(sr),
+                                           _ptr(si)))
+        return sr, si
+
+    def estimate_error(self, fidx, tidx):
+        nsol = 3 if tidx < 0 else 2
+        err = np.zeros((nsol - 1) * self.nt)
+        eta = np.zeros(nsol * self.nt)
+        _check(lib().emg_estimate_error(self._h, int(fidx), int(tidx), _ptr(err), _ptr(eta)))
+        return err.reshape(nsol - 1, self.nt), eta.reshape(nsol, self.nt)
+
+    def interpolate_fields(self, target, fidx, pts, tets):
+        pts = _f64(pts).reshape(-1, 3)
+        out = np.zeros(pts.shape[0] * 12)
+        _check(lib().emg_interpolate_fields(self._h, int(target), int(fidx), pts.shape[0], _ptr(pts),
+                                            _ptr(_i32(tets)), _ptr(out)))
+        o = out.reshape(-1, 6, 2)
+        z = o[..., 0] + 1j * o[..., 1]
+        return z[:, :3], z[:, 3:]
+
+    # -- batched fast path ----------------------------------------------------------------
+    @staticmethod
+    def _opts(rtol, max_it, use_guess, inner_fp32, restart):
+        return BlockOpts(float(rtol), int(max_it), int(use_guess), int(inner_fp32), int(restart))
+
+    def solve_block(self, freqs, rhs, x0=None, rtol=1e-8, max_it=100, inner_fp32=True, restart=30):
+        """rhs: (n, k) complex -- the reference's s = s_re + i s_im per column.
+        Returns (x (n, k) complex = e_re + i e_im, list of SolveInfo)."""
+        freqs = _f64(freqs)
+        k = freqs.size
+        r = np.ascontiguousarray(np.asarray(rhs, dtype=np.complex128).reshape(self.ne, k))
+        x = np.zeros((self.ne, k), dtype=np.complex128) if x0 is None else np.ascontiguousarray(
+            np.asarray(x0, dtype=np.complex128).reshape(self.ne, k))
+        infos = (SolveInfo * k)()
+        o = self._opts(rtol, max_it, x0 is not None, inner_fp32, restart)
+        rc = lib().emg_solve_block(self._h, k, _ptr(freqs), _ptr(r.view(np.float64)), _ptr(x.view(np.float64)),
+                                   C.byref(o), C.cast(infos, C.c_void_p))
+        _check(rc)
+        return x, list(infos)
+
+    def solve_block_dev(self, freqs, rhs_ptr, x_ptr, rtol=1e-8, max_it=100, use_guess=False, inner_fp32=True,
+                        restart=30):
+        freqs = _f64(freqs)
+        k = freqs.size
+        infos = (SolveInfo * k)()
+        o = self._opts(rtol, max_it, use_guess, inner_fp32, restart)
+        _check(lib().emg_solve_block_dev(self._h, k, _ptr(freqs), C.c_void_p(rhs_ptr), C.c_void_p(x_ptr),
+                                         C.byref(o), C.cast(infos, C.c_void_p)))
+        return list(infos)
+
+    def spmv_complex_dev(self, omegas, x_ptr, y_ptr, conj_out=False):
+        om = _f64(omegas)
+        _check(lib().emg_spmv_complex_dev(self._h, om.size, _ptr(om), C.c_void_p(x_ptr), C.c_void_p(y_ptr),
+                                          int(conj_out)))
+
+    def last_kernel_ms(self, name):
+        v = C.c_double()
+        _check(lib().emg_last_kernel_ms(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def synchronize(self):
+        _check(lib().emg_stream_synchronize(self._h))

@@ -1,0 +1,34 @@
+// Host AMG hierarchy (emg_amg.cpp).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "emg_internal.h"
+
+namespace emg {
+
+struct AmgParams {
+  double theta = 0.25;
+  int pmax = 4;
+  int max_coarse = 200;
+  int max_levels = 25;
+  uint64_t seed = 12345;
+};
+
+struct HostLevel {
+  HCsr A;     // level operator (two parts)
+  HCsr P, R;  // interpolation and restriction (single part)
+};
+
+struct HostAmg {
+  std::vector<HostLevel> lv;  // all levels but the coarsest
+  HCsr coarse;                // coarsest operator (two parts)
+};
+
+HCsr transpose(const HCsr &A);
+HCsr spgemm(const HCsr &A, const HCsr &B);
+void amg_build(const HCsr &A0, double w_ref, const AmgParams &prm, HostAmg &out);
+void coarse_inverse(const HCsr &A, double w, std::vector<double> &X);
+
+}  // namespace emg

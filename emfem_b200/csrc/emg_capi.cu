@@ -1,0 +1,1149 @@
+// C ABI of emfem_b200 (include/emfem_b200.h).  Each entry point validates its
+// arguments, runs the host/device work on the context's stream and converts
+// exceptions into status codes with a thread-local message.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <array>
+
+#include "emg_internal.h"
+#include "emg_kernels.cuh"
+#include "emg_linalg.h"
+#include "emg_solver.h"
+
+namespace emg {
+
+static thread_local std::string g_last_error;
+
+void fail(int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw Error(code, buf);
+}
+
+void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    fail(e == cudaErrorMemoryAllocation ? EMG_ERR_NOMEM : EMG_ERR_CUDA, "%s failed at %s:%d: %s", what, file, line,
+         cudaGetErrorString(e));
+  }
+}
+
+// launchers defined in emg_estimate.cu
+void launch_estimate(Context &c, double omega, int nsol, const double *const *sol_dev, double *eta_dev,
+                     double *err_dev, double *scratch_vol, double *scratch_fe);
+void launch_rhs_mt(Context &c, int k, const double *omega_dev, const double *bv_dev, double *s_dev);
+
+struct Workspace {
+  Fcg<double> fcg64;
+  Fcg<float> fcg32;
+  Fgmres gm;
+  DBuf<double> vec_a, vec_b;       // host<->device staging of complex block vectors
+  DBuf<float> f_in, f_out;         // FP32 inner vectors
+  DBuf<double> est_vol, est_fe, est_eta, est_err;
+  DBuf<double> bvals, omega_k, omega_cols;
+  // plain path: hierarchy of B(w) for the assembled frequency (create_pc)
+  Ams<double> pams64;
+  // batched path: two-part hierarchy valid for every frequency of a block
+  bool block_ready64 = false, block_ready32 = false;
+  Ams<double> bams64;
+  Ams<float> bams32;
+};
+
+Context::Context() : ws(new Workspace()) {}
+Context::~Context() {
+  ws.reset();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+static void need(bool cond, int code, const char *msg) {
+  if (!cond) fail(code, "%s", msg);
+}
+
+// ---------------------------------------------------------------------------
+// options (process_options, src/em_ctx.cc:100-175)
+// ---------------------------------------------------------------------------
+static bool is_number(const std::string &s) {
+  if (s.empty()) return false;
+  char *end = nullptr;
+  std::strtod(s.c_str(), &end);
+  return end && *end == '\0';
+}
+
+static void parse_options(Options &o, const std::string &text, std::vector<std::string> &ignored) {
+  std::vector<std::string> tok;
+  std::istringstream ls(text);
+  std::string line;
+  while (std::getline(ls, line)) {
+    size_t h = line.find('#');
+    if (h != std::string::npos) line.erase(h);
+    std::istringstream ws(line);
+    std::string t;
+    while (ws >> t) tok.push_back(t);
+  }
+  auto geti = [](const std::string &k, const std::string &v) {
+    if (!is_number(v)) fail(EMG_ERR_OPTION, "option %s expects a number, got '%s'", k.c_str(), v.c_str());
+    return (int)std::lround(std::strtod(v.c_str(), nullptr));
+  };
+  auto getr = [](const std::string &k, const std::string &v) {
+    if (!is_number(v)) fail(EMG_ERR_OPTION, "option %s expects a number, got '%s'", k.c_str(), v.c_str());
+    return std::strtod(v.c_str(), nullptr);
+  };
+  auto elist = [](const std::string &k, const std::string &v, std::initializer_list<const char *> names) {
+    int i = 0;
+    for (const char *n : names) {
+      if (v == n) return i;
+      ++i;
+    }
+    fail(EMG_ERR_OPTION, "option %s: unknown value '%s'", k.c_str(), v.c_str());
+  };
+  auto getb = [](const std::string &v) { return !(v == "0" || v == "false" || v == "FALSE" || v == "no"); };
+  for (size_t i = 0; i < tok.size(); ++i) {
+    const std::string &k = tok[i];
+    if (k.size() < 2 || k[0] != '-' || is_number(k)) fail(EMG_ERR_OPTION, "unexpected token '%s'", k.c_str());
+    std::string v;
+    if (i + 1 < tok.size() && (tok[i + 1][0] != '-' || is_number(tok[i + 1]))) v = tok[++i];
+    std::string key = k.substr(1);
+    if (key == "iprefix") o.iprefix = v;
+    else if (key == "oprefix") o.oprefix = v;
+    else if (key == "n_groups") o.n_groups = geti(k, v);
+    else if (key == "max_tx_edge_length") o.max_tx_edge_length = getr(k, v);
+    else if (key == "max_rx_edge_length") o.max_rx_edge_length = getr(k, v);
+    else if (key == "mesh_format") o.mesh_format = elist(k, v, {"mdl", "mesh"});
+    else if (key == "inner_pc_type") o.inner_pc_type = elist(k, v, {"mixed", "ams", "direct"});
+    else if (key == "pc_threshold") o.pc_threshold = geti(k, v);
+    else if (key == "direct_solver_type") o.direct_solver_type = elist(k, v, {"mumps", "superlu_dist"});
+    else if (key == "K_max_it") o.K_max_it = geti(k, v);
+    else if (key == "e_rtol") o.e_rtol = getr(k, v);
+    else if (key == "dual_rtol") o.dual_rtol = getr(k, v);
+    else if (key == "max_adaptive_refinements") o.max_adaptive_refinements = geti(k, v);
+    else if (key == "n_uniform_refinements") o.n_uniform_refinements = geti(k, v);
+    else if (key == "max_dofs") o.max_dofs = geti(k, v);
+    else if (key == "refine_fraction") o.refine_fraction = getr(k, v);
+    else if (key == "refine_strategy") o.refine_strategy = elist(k, v, {"fixed_number", "fixed_fraction"});
+    else if (key == "save_mesh") o.save_mesh = v.empty() ? 1 : getb(v);
+    else if (key == "n_tx_divisions") o.n_tx_divisions = geti(k, v);
+    else if (key == "options_file") ;
+    // A_ (outer) and B_ (inner) prefixes: the subset the GPU solver implements
+    else if (key == "A_ksp_gmres_restart") o.gmres_restart = geti(k, v);
+    else if (key == "B_ksp_rtol") o.inner_rtol = getr(k, v);
+    else if (key == "B_ksp_max_it") o.inner_max_it = geti(k, v);
+    else if (key == "B_ksp_fcg_mmax") o.fcg_mmax = geti(k, v);
+    else if (key == "B_pc_hypre_ams_cycle_type") {
+      int ct = geti(k, v);
+      if (ct == 13) o.ams_cycle = "034515430";
+      else if (ct == 11) o.ams_cycle = "013454310";
+      else fail(EMG_ERR_OPTION, "AMS cycle type %d is not implemented (11 and 13 are)", ct);
+    } else if (key == "B_pc_hypre_ams_relax_times") o.ams_relax_times = geti(k, v);
+    else if (key == "B_pc_hypre_ams_relax_weight") o.ams_relax_weight = getr(k, v);
+    else if (key == "B_pc_hypre_ams_amg_alpha_theta" || key == "B_pc_hypre_ams_amg_beta_theta") o.amg_theta = getr(k, v);
+    // emg_* keys of this implementation
+    else if (key == "emg_inner_precision") o.inner_fp32 = elist(k, v, {"fp64", "fp32"});
+    else if (key == "emg_amg_max_coarse") o.amg_max_coarse = geti(k, v);
+    else if (key == "emg_amg_max_levels") o.amg_max_levels = geti(k, v);
+    else if (key == "emg_amg_relax_times") o.amg_relax_times = geti(k, v);
+    else if (key == "emg_amg_pmax") o.amg_pmax = geti(k, v);
+    else if (key == "emg_graphs") o.graphs = v.empty() ? 1 : getb(v);
+    else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
+    else if (key.rfind("A_", 0) == 0 || key.rfind("B_", 0) == 0) ignored.push_back(k);
+    else fail(EMG_ERR_OPTION, "unknown option %s", k.c_str());
+  }
+  if (o.gmres_restart < 1 || o.gmres_restart > 32) fail(EMG_ERR_OPTION, "A_ksp_gmres_restart must be in [1, 32]");
+  if (o.fcg_mmax < 1 || o.fcg_mmax > 30) fail(EMG_ERR_OPTION, "B_ksp_fcg_mmax must be in [1, 30]");
+  if (o.ams_relax_times < 1 || o.amg_relax_times < 1) fail(EMG_ERR_OPTION, "relax times must be >= 1");
+}
+
+// ---------------------------------------------------------------------------
+// host FE helpers for the sparse RHS pieces (dipoles, receivers, boundary
+// values): gradients of the barycentric coordinates of one tet
+// ---------------------------------------------------------------------------
+struct HostTet {
+  double x[4][3], gr[4][3], vol;
+  int v[4];
+};
+
+static void host_tet(const Context &c, int t, HostTet &h) {
+  for (int i = 0; i < 4; ++i) {
+    h.v[i] = c.h_tets[4 * (size_t)t + i];
+    for (int d = 0; d < 3; ++d) h.x[i][d] = c.h_pts[3 * (size_t)h.v[i] + d];
+  }
+  double e1[3], e2[3], e3[3];
+  for (int d = 0; d < 3; ++d) {
+    e1[d] = h.x[1][d] - h.x[0][d];
+    e2[d] = h.x[2][d] - h.x[0][d];
+    e3[d] = h.x[3][d] - h.x[0][d];
+  }
+  double c23[3] = {e2[1] * e3[2] - e2[2] * e3[1], e2[2] * e3[0] - e2[0] * e3[2], e2[0] * e3[1] - e2[1] * e3[0]};
+  double c31[3] = {e3[1] * e1[2] - e3[2] * e1[1], e3[2] * e1[0] - e3[0] * e1[2], e3[0] * e1[1] - e3[1] * e1[0]};
+  double c12[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+  double det = e1[0] * c23[0] + e1[1] * c23[1] + e1[2] * c23[2];
+  for (int d = 0; d < 3; ++d) {
+    h.gr[1][d] = c23[d] / det;
+    h.gr[2][d] = c31[d] / det;
+    h.gr[3][d] = c12[d] / det;
+    h.gr[0][d] = -(h.gr[1][d] + h.gr[2][d] + h.gr[3][d]);
+  }
+  h.vol = det / 6.0;
+}
+
+static double host_lambda(const HostTet &h, int p, const double *y) {
+  return 1.0 + h.gr[p][0] * (y[0] - h.x[p][0]) + h.gr[p][1] * (y[1] - h.x[p][1]) + h.gr[p][2] * (y[2] - h.x[p][2]);
+}
+
+// local edge i of tet t: value of phi_i at y (global orientation lower->higher id)
+static void host_phi(const Context &c, const HostTet &h, int t, int i, const double *y, double out[3], int *ge) {
+  int e = c.h_t2e[6 * (size_t)t + i];
+  int a = c.h_edges[2 * (size_t)e], b = c.h_edges[2 * (size_t)e + 1];
+  int la = -1, lb = -1;
+  for (int q = 0; q < 4; ++q) {
+    if (h.v[q] == a) la = q;
+    if (h.v[q] == b) lb = q;
+  }
+  if (la < 0 || lb < 0) fail(EMG_ERR_USER, "tet %d does not contain its edge %d", t, e);
+  double l0 = host_lambda(h, la, y), l1 = host_lambda(h, lb, y);
+  for (int d = 0; d < 3; ++d) out[d] = l0 * h.gr[lb][d] - l1 * h.gr[la][d];
+  *ge = e;
+}
+
+// 1-D layered plane wave (src/em_pw.h:6-139)
+struct PlaneWave1D {
+  typedef std::complex<double> zc;
+  int nlay = 0;
+  double omega = 0;
+  std::vector<double> ztop, lsig;
+  std::vector<zc> a, b, cc, d;
+  void init(const double *zt, const double *ls, int n, double freq) {
+    const zc I(0, 1);
+    nlay = n;
+    ztop.assign(zt, zt + n);
+    lsig.assign(ls, ls + n);
+    omega = 2 * PI * freq;
+    std::vector<zc> kk(n + 1), Rp(n + 1, 0.0), ex(n + 1, 0.0);
+    for (int i = 1; i <= n; ++i) kk[i] = std::sqrt(-I * omega * MU * lsig[i - 1]);
+    kk[0] = std::sqrt(-I * omega * MU * lsig[0]);
+    for (int i = 1; i <= n - 1; ++i) ex[i] = std::exp(-kk[i] * (ztop[i] - ztop[i - 1]));
+    for (int i = n - 1; i >= 1; --i) {
+      zc gm = (-I * omega * MU * (lsig[i - 1] - lsig[i])) / ((kk[i] + kk[i + 1]) * (kk[i] + kk[i + 1]));
+      zc rj = Rp[i + 1] * ex[i + 1];
+      Rp[i] = (gm + rj) / (1.0 + gm * rj) * ex[i];
+    }
+    a.assign(n + 1, 0.0);
+    b.assign(n + 1, 0.0);
+    cc.assign(n + 1, 0.0);
+    d.assign(n + 1, 0.0);
+    a[0] = 1.0;
+    cc[0] = 1.0;
+    for (int i = 1; i <= n; ++i) {
+      zc At = a[i - 1] + b[i - 1] * ex[i - 1];
+      b[i] = At / (1.0 + Rp[i] * ex[i]);
+      a[i] = b[i] * Rp[i];
+      At = cc[i - 1] + d[i - 1] * ex[i - 1];
+      d[i] = At / (1.0 - Rp[i] * ex[i]);
+      cc[i] = -d[i] * Rp[i];
+    }
+  }
+  void field(double z, zc eh[4]) const {
+    const zc I(0, 1);
+    int il = 0;
+    for (int i = nlay - 1; i >= 0; --i)
+      if (z >= ztop[i]) { il = i; break; }
+    zc kk = std::sqrt(-I * omega * MU * lsig[il]);
+    zc ep = 0.0, epd = 0.0;
+    zc em = std::exp(-kk * (z - ztop[il]));
+    zc emd = -kk * em;
+    if (il != nlay - 1) {
+      ep = std::exp(kk * (z - ztop[il + 1]));
+      epd = kk * ep;
+    }
+    eh[0] = a[il + 1] * ep + b[il + 1] * em;
+    eh[1] = (a[il + 1] * epd + b[il + 1] * emd) / (I * MU * omega);
+    eh[2] = (cc[il + 1] * epd + d[il + 1] * emd) / lsig[il];
+    eh[3] = cc[il + 1] * ep + d[il + 1] * em;
+    for (int i = 0; i < 4; ++i)
+      if (std::abs(eh[i]) < 1E-80) eh[i] = 0.0;
+  }
+};
+
+// calculate_boundary_values (src/em_fwd.cc:402-486): Dirichlet value of every
+// boundary edge (first encounter in ascending tet order wins)
+static void boundary_values(Context &c, double freq, int mode, std::vector<std::complex<double>> &bv,
+                            const std::vector<unsigned char> &bdr_cell) {
+  typedef std::complex<double> zc;
+  need(!c.bg_nlay.empty(), EMG_ERR_STATE, "MT right-hand side needs emg_set_background first");
+  PlaneWave1D pw[4];
+  for (int q = 0; q < 4; ++q) pw[q].init(&c.bg_ztop[q * c.bg_maxl], &c.bg_lsig[q * c.bg_maxl], c.bg_nlay[q], freq);
+  const double *tc = c.bg_corners.data();
+  auto T = [&](int q, int d) { return tc[3 * q + d]; };
+  bv.assign(c.ne, zc(0));
+  std::vector<char> have(c.ne, 0);
+  for (int t = 0; t < c.nt; ++t) {
+    if (!bdr_cell[t]) continue;
+    HostTet h;
+    host_tet(c, t, h);
+    for (int i = 0; i < 6; ++i) {
+      int e = c.h_t2e[6 * (size_t)t + i];
+      if (!c.h_ebdr[e] || have[e]) continue;
+      const double *p0 = &c.h_pts[3 * (size_t)c.h_edges[2 * (size_t)e]];
+      const double *p1 = &c.h_pts[3 * (size_t)c.h_edges[2 * (size_t)e + 1]];
+      double ec[3], ed[3];
+      for (int d = 0; d < 3; ++d) {
+        ec[d] = (p0[d] + p1[d]) / 2.0;
+        ed[d] = p1[d] - p0[d];
+      }
+      double co[4];
+      if (std::fabs(ec[0] - T(0, 0)) < EPS) {
+        double w = (1.0 - std::cos(PI * (ec[1] - T(0, 1)) / (T(2, 1) - T(0, 1)))) / 2.0;
+        co[0] = 1.0 - w; co[1] = 0.0; co[2] = 0.0; co[3] = w;
+      } else if (std::fabs(ec[1] - T(0, 1)) < EPS) {
+        double w = (1.0 - std::cos(PI * (ec[0] - T(0, 0)) / (T(2, 0) - T(0, 0)))) / 2.0;
+        co[0] = 1.0 - w; co[1] = w; co[2] = 0.0; co[3] = 0.0;
+      } else if (std::fabs(ec[0] - T(2, 0)) < EPS) {
+        double w = (1.0 - std::cos(PI * (ec[1] - T(0, 1)) / (T(2, 1) - T(0, 1)))) / 2.0;
+        co[0] = 0.0; co[1] = 1.0 - w; co[2] = w; co[3] = 0.0;
+      } else if (std::fabs(ec[1] - T(2, 1)) < EPS) {
+        double w = (1.0 - std::cos(PI * (ec[0] - T(0, 0)) / (T(2, 0) - T(0, 0)))) / 2.0;
+        co[0] = 0.0; co[1] = 0.0; co[2] = w; co[3] = 1.0 - w;
+      } else {
+        double area = (T(2, 0) - T(0, 0)) * (T(2, 1) - T(0, 1));
+        co[0] = ((T(2, 0) - ec[0]) * (T(2, 1) - ec[1])) / area;
+        co[1] = ((ec[0] - T(3, 0)) * (T(3, 1) - ec[1])) / area;
+        co[2] = ((ec[0] - T(0, 0)) * (ec[1] - T(0, 1))) / area;
+        co[3] = ((T(1, 0) - ec[0]) * (ec[1] - T(1, 1))) / area;
+      }
+      zc ep[3] = {0.0, 0.0, 0.0};
+      for (int q = 0; q < 4; ++q) {
+        zc eh[4];
+        pw[q].field(ec[2], eh);
+        if (mode == EMG_SOL_MT_XY) ep[0] += co[q] * std::conj(eh[0]);
+        else if (mode == EMG_SOL_MT_YX) ep[1] += co[q] * std::conj(eh[2]);
+      }
+      double phi[3];
+      int ge;
+      host_phi(c, h, t, i, ec, phi, &ge);
+      zc num = ed[0] * ep[0] + ed[1] * ep[1] + ed[2] * ep[2];
+      zc dof = num / (ed[0] * phi[0] + ed[1] * phi[1] + ed[2] * phi[2]);
+      have[e] = 1;
+      bv[e] = std::abs(dof) > 1E-13 ? dof : zc(0.0);
+    }
+  }
+}
+
+static DBuf<double> &slot_buf(Context &c, int target) {
+  need(target == EMG_SOL_MT_XY || target == EMG_SOL_MT_YX || target == EMG_SOL_CSEM || target == EMG_SOL_DUAL,
+       EMG_ERR_ARG, "unknown solution slot");
+  DBuf<double> &b = c.sol[target];
+  if (b.n != (size_t)c.ne * 2) {
+    b.alloc((size_t)c.ne * 2);
+    b.zero(c.stream);
+  }
+  return b;
+}
+
+static std::vector<double> interleave(const double *re, const double *im, int n) {
+  std::vector<double> v((size_t)n * 2);
+  for (int i = 0; i < n; ++i) {
+    v[2 * (size_t)i] = re ? re[i] : 0.0;
+    v[2 * (size_t)i + 1] = im ? im[i] : 0.0;
+  }
+  return v;
+}
+
+}  // namespace emg
+
+using namespace emg;
+
+struct emg_context : public emg::Context {};
+
+#define EMG_API_BEGIN try {
+#define EMG_API_END                                  \
+  }                                                  \
+  catch (const emg::Error &e) {                      \
+    emg::g_last_error = e.what();                    \
+    return e.code;                                   \
+  }                                                  \
+  catch (const std::exception &e) {                  \
+    emg::g_last_error = e.what();                    \
+    return EMG_ERR_USER;                             \
+  }                                                  \
+  return EMG_OK;
+
+extern "C" {
+
+const char *emg_last_error(void) { return emg::g_last_error.c_str(); }
+const char *emg_version(void) { return "emfem_b200 0.1 (sm_100a)"; }
+
+int emg_create_context(emg_context **ctx, int device) {
+  EMG_API_BEGIN
+  need(ctx != nullptr, EMG_ERR_ARG, "null context pointer");
+  if (device < 0) {  // host-only context: options and host-side helpers, no GPU work
+    emg_context *c = new emg_context();
+    c->device = -1;
+    *ctx = c;
+    return EMG_OK;
+  }
+  int ndev = 0;
+  EMG_CUDA(cudaGetDeviceCount(&ndev));
+  need(device >= 0 && device < ndev, EMG_ERR_ARG, "no such CUDA device");
+  EMG_CUDA(cudaSetDevice(device));
+  emg_context *c = new emg_context();
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    check_cuda(e, "cudaStreamCreate", __FILE__, __LINE__);
+  }
+  *ctx = c;
+  EMG_API_END
+}
+
+int emg_destroy_context(emg_context *ctx) {
+  EMG_API_BEGIN
+  if (!ctx) return EMG_OK;
+  if (ctx->device >= 0) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  delete ctx;
+  EMG_API_END
+}
+
+int emg_process_options(emg_context *ctx, const char *text) {
+  EMG_API_BEGIN
+  need(ctx && text, EMG_ERR_ARG, "null argument");
+  Options o = ctx->opt;
+  std::vector<std::string> ignored;
+  parse_options(o, text, ignored);
+  ctx->opt = o;
+  for (auto &k : ignored)
+    if (o.verbose) fprintf(stderr, "emfem_b200: option %s is not used by the GPU solver\n", k.c_str());
+  EMG_API_END
+}
+
+int emg_get_option(emg_context *ctx, const char *key, double *value) {
+  EMG_API_BEGIN
+  need(ctx && key && value, EMG_ERR_ARG, "null argument");
+  std::string k = key[0] == '-' ? key + 1 : key;
+  const Options &o = ctx->opt;
+  if (k == "K_max_it") *value = o.K_max_it;
+  else if (k == "e_rtol") *value = o.e_rtol;
+  else if (k == "dual_rtol") *value = o.dual_rtol;
+  else if (k == "inner_pc_type") *value = o.inner_pc_type;
+  else if (k == "pc_threshold") *value = o.pc_threshold;
+  else if (k == "n_tx_divisions") *value = o.n_tx_divisions;
+  else if (k == "refine_fraction") *value = o.refine_fraction;
+  else if (k == "refine_strategy") *value = o.refine_strategy;
+  else if (k == "max_adaptive_refinements") *value = o.max_adaptive_refinements;
+  else if (k == "n_uniform_refinements") *value = o.n_uniform_refinements;
+  else if (k == "max_dofs") *value = o.max_dofs;
+  else if (k == "save_mesh") *value = o.save_mesh;
+  else if (k == "n_groups") *value = o.n_groups;
+  else if (k == "A_ksp_gmres_restart") *value = o.gmres_restart;
+  else if (k == "B_ksp_rtol") *value = o.inner_rtol;
+  else if (k == "B_ksp_max_it") *value = o.inner_max_it;
+  else if (k == "B_ksp_fcg_mmax") *value = o.fcg_mmax;
+  else if (k == "emg_inner_precision") *value = o.inner_fp32;
+  else fail(EMG_ERR_OPTION, "unknown option %s", key);
+  EMG_API_END
+}
+
+int emg_set_mesh(emg_context *c, int nv, const double *pts, int nt, const int *tets, const int *attr, int ne,
+                 const int *edges, const int *t2e, const int *nbr, const int *non, const unsigned char *ebdr) {
+  EMG_API_BEGIN
+  need(c && pts && tets && attr && edges && t2e && nbr && non && ebdr, EMG_ERR_ARG, "null mesh array");
+  need(nv > 0 && nt > 0 && ne > 0, EMG_ERR_ARG, "empty mesh");
+  need(c->device >= 0, EMG_ERR_STATE, "host-only context has no device");
+  EMG_CUDA(cudaSetDevice(c->device));
+  for (long i = 0; i < 4L * nt; ++i)
+    need(tets[i] >= 0 && tets[i] < nv, EMG_ERR_ARG, "tetrahedronlist index out of range");
+  for (long i = 0; i < 6L * nt; ++i) need(t2e[i] >= 0 && t2e[i] < ne, EMG_ERR_ARG, "tet2edgelist index out of range");
+  for (long i = 0; i < 2L * ne; ++i) need(edges[i] >= 0 && edges[i] < nv, EMG_ERR_ARG, "edgelist index out of range");
+  for (long i = 0; i < ne; ++i) need(edges[2 * i] < edges[2 * i + 1], EMG_ERR_ARG, "edgelist endpoints must be sorted ascending");
+  for (long i = 0; i < 4L * nt; ++i) {
+    need(nbr[i] >= -1 && nbr[i] < nt, EMG_ERR_ARG, "neighborlist index out of range");
+    need(nbr[i] < 0 || (non[i] >= 0 && non[i] < 4), EMG_ERR_ARG, "tet_non index out of range");
+  }
+  c->nv = nv;
+  c->nt = nt;
+  c->ne = ne;
+  c->h_pts.assign(pts, pts + 3L * nv);
+  c->h_tets.assign(tets, tets + 4L * nt);
+  c->h_attr.assign(attr, attr + nt);
+  c->h_edges.assign(edges, edges + 2L * ne);
+  c->h_t2e.assign(t2e, t2e + 6L * nt);
+  c->h_nbr.assign(nbr, nbr + 4L * nt);
+  c->h_non.assign(non, non + 4L * nt);
+  c->h_ebdr.assign(ebdr, ebdr + ne);
+  c->pts.upload(c->h_pts, c->stream);
+  c->tets.upload(c->h_tets, c->stream);
+  c->attr.upload(c->h_attr, c->stream);
+  c->edges.upload(c->h_edges, c->stream);
+  c->t2e.upload(c->h_t2e, c->stream);
+  c->nbr.upload(c->h_nbr, c->stream);
+  c->non.upload(c->h_non, c->stream);
+  c->ebdr.upload(c->h_ebdr, c->stream);
+  canonicalize(*c);
+  c->have_ls = false;
+  c->assembled = false;
+  c->have_pc = false;
+  c->ws->block_ready64 = c->ws->block_ready32 = false;
+  c->sol.clear();
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+int emg_set_model(emg_context *c, int aniso_form, int n_rho, int ncol, const double *rho) {
+  EMG_API_BEGIN
+  need(c && rho && n_rho > 0, EMG_ERR_ARG, "bad model");
+  static const int need_cols[4] = {1, 2, 3, 6};
+  if (aniso_form < 0 || aniso_form > 3) fail(EMG_ERR_USER, "Unsupported anisotropy form %d.", aniso_form);
+  need(ncol >= need_cols[aniso_form], EMG_ERR_ARG, "too few resistivity columns for the anisotropy form");
+  if (c->nt) {
+    for (int a : c->h_attr) need(a >= 0 && a < n_rho, EMG_ERR_ARG, "tet attribute beyond the resistivity table");
+  }
+  c->aniso_form = aniso_form;
+  c->nrho = n_rho;
+  c->ncol = ncol;
+  c->rho.assign(rho, rho + (size_t)n_rho * ncol);
+  sigma_table(aniso_form, n_rho, ncol, rho, c->h_sigma_tab);
+  if (c->device >= 0) c->sigma_tab.upload(c->h_sigma_tab, c->stream);
+  c->assembled = false;
+  c->ws->block_ready64 = c->ws->block_ready32 = false;
+  if (c->device >= 0) EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+int emg_set_frequencies(emg_context *c, int n, const double *f) {
+  EMG_API_BEGIN
+  need(c && (n == 0 || f), EMG_ERR_ARG, "bad frequencies");
+  c->freqs.assign(f, f + n);
+  EMG_API_END
+}
+
+int emg_create_linear_system(emg_context *c, int tidx) {
+  EMG_API_BEGIN
+  need(c && c->nt > 0, EMG_ERR_STATE, "create_linear_system before emg_set_mesh");
+  EMG_CUDA(cudaSetDevice(c->device));
+  c->tidx = tidx;
+  build_sparsity(*c);
+  build_vertex_pattern(*c);
+  build_slot_maps(*c);
+  c->have_ls = true;
+  c->assembled = false;
+  c->have_pc = false;
+  c->ws->block_ready64 = c->ws->block_ready32 = false;
+  // named solution vectors (src/em_fwd.cc:267-280)
+  c->sol.clear();
+  slot_buf(*c, EMG_SOL_DUAL);
+  if (tidx < 0) {
+    slot_buf(*c, EMG_SOL_MT_XY);
+    slot_buf(*c, EMG_SOL_MT_YX);
+  } else {
+    slot_buf(*c, EMG_SOL_CSEM);
+  }
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+int emg_destroy_linear_system(emg_context *c) {
+  EMG_API_BEGIN
+  need(c != nullptr, EMG_ERR_ARG, "null context");
+  c->Cv.release();
+  c->Msv.release();
+  c->slot.release();
+  c->vslot.release();
+  c->rp.release();
+  c->ci.release();
+  c->sol.clear();
+  c->have_ls = c->assembled = c->have_pc = false;
+  c->ws->block_ready64 = c->ws->block_ready32 = false;
+  EMG_API_END
+}
+
+int emg_get_sparsity(emg_context *c, long *nnz, int *rptr, int *cidx) {
+  EMG_API_BEGIN
+  need(c && nnz, EMG_ERR_ARG, "null argument");
+  need(c->have_ls, EMG_ERR_STATE, "no linear system");
+  *nnz = c->nnz;
+  if (rptr) std::copy(c->h_rp.begin(), c->h_rp.end(), rptr);
+  if (cidx) std::copy(c->h_ci.begin(), c->h_ci.end(), cidx);
+  EMG_API_END
+}
+
+int emg_assemble_matrix(emg_context *c, int fidx) {
+  EMG_API_BEGIN
+  need(c && c->have_ls, EMG_ERR_STATE, "assemble_matrix before create_linear_system");
+  need(c->nrho > 0, EMG_ERR_STATE, "assemble_matrix before emg_set_model");
+  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
+  EMG_CUDA(cudaSetDevice(c->device));
+  c->omega = 2 * PI * c->freqs[fidx];
+  cudaEvent_t e0, e1;
+  EMG_CUDA(cudaEventCreate(&e0));
+  EMG_CUDA(cudaEventCreate(&e1));
+  EMG_CUDA(cudaEventRecord(e0, c->stream));
+  assemble_edge(*c);
+  EMG_CUDA(cudaEventRecord(e1, c->stream));
+  EMG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  EMG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  c->kernel_ms["assemble"] = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->assembled = true;
+  c->have_pc = false;
+  c->ws->block_ready64 = c->ws->block_ready32 = false;
+  EMG_API_END
+}
+
+__global__ static void scale_copy_kernel(long n, const double *a, double w, double *b) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = w * a[i];
+}
+
+int emg_get_matrices(emg_context *c, double *C, double *M, unsigned char *bdr) {
+  EMG_API_BEGIN
+  need(c && c->assembled, EMG_ERR_STATE, "matrices not assembled");
+  EMG_CUDA(cudaSetDevice(c->device));
+  if (C) c->Cv.download(C, c->nnz, c->stream);
+  if (M) {
+    DBuf<double> tmp(c->nnz);
+    scale_copy_kernel<<<(unsigned)((c->nnz + 255) / 256), 256, 0, c->stream>>>(c->nnz, c->Msv.p, c->omega, tmp.p);
+    EMG_LAUNCH_CHECK();
+    tmp.download(M, c->nnz, c->stream);
+    EMG_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  if (bdr) c->bdr_cell.download(bdr, c->nt, c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+int emg_create_pc(emg_context *c) {
+  EMG_API_BEGIN
+  need(c && c->assembled, EMG_ERR_STATE, "create_pc before assemble_matrix");
+  EMG_CUDA(cudaSetDevice(c->device));
+  cudaEvent_t e0, e1;
+  EMG_CUDA(cudaEventCreate(&e0));
+  EMG_CUDA(cudaEventCreate(&e1));
+  EMG_CUDA(cudaEventRecord(e0, c->stream));
+  ams_setup<double>(*c, c->ws->pams64, true, c->omega, c->omega);
+  c->ws->pams64.set_columns({c->omega, c->omega}, c->stream);
+  EMG_CUDA(cudaEventRecord(e1, c->stream));
+  EMG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  EMG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  c->kernel_ms["create_pc"] = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->pc_omega = c->omega;
+  c->have_pc = true;
+  EMG_API_END
+}
+
+int emg_destroy_pc(emg_context *c) {
+  EMG_API_BEGIN
+  need(c != nullptr, EMG_ERR_ARG, "null context");
+  c->ws->pams64 = Ams<double>();
+  c->have_pc = false;
+  EMG_API_END
+}
+
+int emg_matshell_mult_a(emg_context *c, const double *x, double *y) {
+  EMG_API_BEGIN
+  need(c && x && y, EMG_ERR_ARG, "null argument");
+  need(c->assembled, EMG_ERR_STATE, "operator not assembled");
+  EMG_CUDA(cudaSetDevice(c->device));
+  const int n = c->ne;
+  std::vector<double> xi = interleave(x, x + n, n);
+  Workspace &w = *c->ws;
+  w.vec_a.upload(xi, c->stream);
+  w.vec_b.alloc((size_t)n * 2);
+  w.omega_k.upload(&c->omega, 1, c->stream);
+  spmm_complex(n, 1, c->rp.p, c->ci.p, c->Cv.p, c->Msv.p, w.omega_k.p, w.vec_a.p, nullptr, w.vec_b.p, false, true,
+               c->stream);
+  std::vector<double> yo((size_t)n * 2);
+  w.vec_b.download(yo.data(), yo.size(), c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; ++i) {
+    y[i] = yo[2 * (size_t)i];
+    y[n + i] = yo[2 * (size_t)i + 1];
+  }
+  EMG_API_END
+}
+
+int emg_pc_apply_b(emg_context *c, const double *b, double *x) {
+  EMG_API_BEGIN
+  need(c && b && x, EMG_ERR_ARG, "null argument");
+  need(c->have_pc, EMG_ERR_STATE, "pc_apply_b before create_pc");
+  EMG_CUDA(cudaSetDevice(c->device));
+  const int n = c->ne;
+  Workspace &w = *c->ws;
+  std::vector<double> bi = interleave(b, b + n, n);
+  w.vec_a.upload(bi, c->stream);
+  w.vec_b.alloc((size_t)n * 2);
+  w.fcg64.mmax = c->opt.fcg_mmax;
+  w.fcg64.solve(w.pams64, w.vec_a.p, w.vec_b.p, c->opt.inner_rtol, c->opt.inner_max_it, c->stream);
+  std::vector<double> xo((size_t)n * 2);
+  w.vec_b.download(xo.data(), xo.size(), c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; ++i) {
+    x[i] = xo[2 * (size_t)i];
+    x[n + i] = xo[2 * (size_t)i + 1];
+  }
+  EMG_API_END
+}
+
+static void fill_info(emg_solve_info *info, const SolveStats &st, long inner, int col) {
+  if (!info) return;
+  info->outer_its = col >= 0 && col < (int)st.col_its.size() ? st.col_its[col] : st.outer_its;
+  info->inner_its = (int)inner;
+  info->true_rel_res = col >= 0 && col < (int)st.true_res.size() ? st.true_res[col] : 0.0;
+  info->reason = (col >= 0 && col < (int)st.converged.size() && !st.converged[col]) ? EMG_DIVERGED_ITS : 0;
+  info->seconds = st.seconds;
+}
+
+int emg_solve_linear_system(emg_context *c, int target, const double *s_re, const double *s_im, int max_it,
+                            double rtol, emg_solve_info *info) {
+  EMG_API_BEGIN
+  need(c && s_re && s_im, EMG_ERR_ARG, "null argument");
+  need(c->have_pc, EMG_ERR_STATE, "solve_linear_system before create_pc");
+  need(max_it > 0 && rtol > 0, EMG_ERR_ARG, "bad tolerances");
+  EMG_CUDA(cudaSetDevice(c->device));
+  const int n = c->ne;
+  Workspace &w = *c->ws;
+  DBuf<double> &x = slot_buf(*c, target);
+  std::vector<double> bi = interleave(s_re, s_im, n);
+  w.vec_a.upload(bi, c->stream);
+  w.gm.k = 1;
+  w.gm.restart = c->opt.gmres_restart;
+  w.gm.omega.upload(&c->omega, 1, c->stream);
+  w.fcg64.mmax = c->opt.fcg_mmax;
+  w.fcg64.total_its = 0;
+  SolveStats st;
+  auto pc = [&](const double *v, double *z) {
+    w.fcg64.solve(w.pams64, v, z, c->opt.inner_rtol, c->opt.inner_max_it, c->stream);
+  };
+  w.gm.solve(*c, w.vec_a.p, x.p, false, rtol, max_it, true, pc, st);
+  fill_info(info, st, w.fcg64.total_its, 0);
+  c->kernel_ms["solve"] = st.seconds * 1e3;
+  if (!st.converged[0]) fail(EMG_DIVERGED_ITS, "FGMRES reached %d iterations at relative residual %.3e", max_it,
+                             st.true_res[0]);
+  EMG_API_END
+}
+
+int emg_get_solution(emg_context *c, int target, double *e_re, double *e_im) {
+  EMG_API_BEGIN
+  need(c && (e_re || e_im), EMG_ERR_ARG, "null argument");
+  need(c->have_ls, EMG_ERR_STATE, "no linear system");
+  EMG_CUDA(cudaSetDevice(c->device));
+  DBuf<double> &x = slot_buf(*c, target);
+  std::vector<double> v((size_t)c->ne * 2);
+  x.download(v.data(), v.size(), c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < c->ne; ++i) {
+    if (e_re) e_re[i] = v[2 * (size_t)i];
+    if (e_im) e_im[i] = v[2 * (size_t)i + 1];
+  }
+  EMG_API_END
+}
+
+int emg_set_solution(emg_context *c, int target, const double *e_re, const double *e_im) {
+  EMG_API_BEGIN
+  need(c && e_re && e_im, EMG_ERR_ARG, "null argument");
+  need(c->have_ls, EMG_ERR_STATE, "no linear system");
+  EMG_CUDA(cudaSetDevice(c->device));
+  DBuf<double> &x = slot_buf(*c, target);
+  std::vector<double> v = interleave(e_re, e_im, c->ne);
+  x.upload(v, c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+int emg_set_background(emg_context *c, const double *corners, const int *nlay, const double *ztop,
+                       const double *lsig, int maxl) {
+  EMG_API_BEGIN
+  need(c && corners && nlay && ztop && lsig && maxl > 0, EMG_ERR_ARG, "bad background model");
+  for (int q = 0; q < 4; ++q) need(nlay[q] >= 1 && nlay[q] <= maxl, EMG_ERR_ARG, "bad layer count");
+  c->bg_corners.assign(corners, corners + 12);
+  c->bg_nlay.assign(nlay, nlay + 4);
+  c->bg_ztop.assign(ztop, ztop + 4 * maxl);
+  c->bg_lsig.assign(lsig, lsig + 4 * maxl);
+  c->bg_maxl = maxl;
+  EMG_API_END
+}
+
+// MT right-hand side for k (frequency, polarisation) columns on the device:
+// boundary values on the host (plane waves), lifting by the GPU kernel.
+static void rhs_mt_block(Context &c, int k, const double *freqs, const int *modes, double *s_dev) {
+  Workspace &w = *c.ws;
+  std::vector<unsigned char> bdr(c.nt);
+  c.bdr_cell.download(bdr.data(), c.nt, c.stream);
+  EMG_CUDA(cudaStreamSynchronize(c.stream));
+  std::vector<double> bv((size_t)c.ne * k * 2, 0.0), om(k);
+  for (int j = 0; j < k; ++j) {
+    std::vector<std::complex<double>> v;
+    boundary_values(c, freqs[j], modes[j], v, bdr);
+    for (int e = 0; e < c.ne; ++e) {
+      bv[2 * ((size_t)e * k + j)] = v[e].real();
+      bv[2 * ((size_t)e * k + j) + 1] = v[e].imag();
+    }
+    om[j] = 2 * PI * freqs[j];
+  }
+  w.bvals.upload(bv, c.stream);
+  w.omega_k.upload(om, c.stream);
+  launch_rhs_mt(c, k, w.omega_k.p, w.bvals.p, s_dev);
+  EMG_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+int emg_assemble_rhs_mt(emg_context *c, int fidx, int mode, double *s_re, double *s_im) {
+  EMG_API_BEGIN
+  need(c && s_re && s_im, EMG_ERR_ARG, "null argument");
+  need(c->assembled, EMG_ERR_STATE, "assemble_rhs_mt before assemble_matrix");
+  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
+  need(mode == EMG_SOL_MT_XY || mode == EMG_SOL_MT_YX, EMG_ERR_ARG, "mode must be XY_POLAR or YX_POLAR");
+  EMG_CUDA(cudaSetDevice(c->device));
+  DBuf<double> s((size_t)c->ne * 2);
+  double f = c->freqs[fidx];
+  rhs_mt_block(*c, 1, &f, &mode, s.p);
+  std::vector<double> v((size_t)c->ne * 2);
+  s.download(v.data(), v.size(), c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < c->ne; ++i) {
+    s_re[i] = v[2 * (size_t)i];
+    s_im[i] = v[2 * (size_t)i + 1];
+  }
+  EMG_API_END
+}
+
+// divide_line_source + assemble_rhs_csem (src/em_fwd.cc:582-671); the cell of
+// every dipole comes from the host mesh's point location.
+int emg_assemble_rhs_csem(emg_context *c, int fidx, const double *tx, const int *dtets, double *s_re,
+                          double *s_im) {
+  EMG_API_BEGIN
+  need(c && tx && dtets && s_re && s_im, EMG_ERR_ARG, "null argument");
+  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
+  const double omega = 2 * PI * c->freqs[fidx];
+  double dir[3] = {std::cos(tx[3] * DTOR) * std::cos(tx[4] * DTOR), std::sin(tx[3] * DTOR) * std::cos(tx[4] * DTOR),
+                   std::sin(tx[4] * DTOR)};
+  double current = tx[5], length = tx[6];
+  std::vector<std::array<double, 3>> pts;
+  std::vector<double> wts;
+  if (std::fabs(length) <= 0.1) {
+    pts.push_back({tx[0], tx[1], tx[2]});
+    wts.push_back(1.0);
+  } else {
+    int nd = c->opt.n_tx_divisions;
+    double A[3] = {tx[0] - dir[0] * length / 2, tx[1] - dir[1] * length / 2, tx[2] - dir[2] * length / 2};
+    for (int i = 0; i < nd; ++i) {
+      double Bp[3] = {A[0] + dir[0] * length / nd, A[1] + dir[1] * length / nd, A[2] + dir[2] * length / nd};
+      pts.push_back({(A[0] + Bp[0]) / 2, (A[1] + Bp[1]) / 2, (A[2] + Bp[2]) / 2});
+      wts.push_back(1.0 / nd);
+      for (int d = 0; d < 3; ++d) A[d] = Bp[d];
+    }
+  }
+  std::fill(s_re, s_re + c->ne, 0.0);
+  std::fill(s_im, s_im + c->ne, 0.0);
+  for (size_t j = 0; j < pts.size(); ++j) {
+    int t = dtets[j];
+    if (t < 0 || t >= c->nt) fail(EMG_ERR_USER, "Transmitter %d is not found in mesh.", (int)j);
+    HostTet h;
+    host_tet(*c, t, h);
+    for (int i = 0; i < 6; ++i) {
+      double phi[3];
+      int ge;
+      host_phi(*c, h, t, i, pts[j].data(), phi, &ge);
+      s_im[ge] += omega * current * (phi[0] * dir[0] + phi[1] * dir[1] + phi[2] * dir[2]) * wts[j];
+    }
+  }
+  EMG_API_END
+}
+
+// assemble_rhs_dual (src/em_fwd.cc:673-717)
+int emg_assemble_rhs_dual(emg_context *c, int nrx, const double *rx, const int *rtets, double *s_re, double *s_im) {
+  EMG_API_BEGIN
+  need(c && rx && rtets && s_re && s_im, EMG_ERR_ARG, "null argument");
+  std::fill(s_re, s_re + c->ne, 0.0);
+  std::fill(s_im, s_im + c->ne, 0.0);
+  for (int r = 0; r < nrx; ++r) {
+    int t = rtets[r];
+    if (t < 0 || t >= c->nt) fail(EMG_ERR_USER, "Receiver %d is not found in mesh.", r);
+    HostTet h;
+    host_tet(*c, t, h);
+    for (int j = 0; j < 6; ++j) {
+      double phi[3];
+      int ge;
+      host_phi(*c, h, t, j, rx + 3 * r, phi, &ge);
+      double v = phi[0] + phi[1] + phi[2];
+      s_re[ge] += v;
+      s_im[ge] += v;
+    }
+  }
+  EMG_API_END
+}
+
+int emg_estimate_error(emg_context *c, int fidx, int tidx, double *err, double *eta_raw) {
+  EMG_API_BEGIN
+  need(c && (err || eta_raw), EMG_ERR_ARG, "null argument");
+  need(c->have_ls && c->nrho > 0, EMG_ERR_STATE, "estimate_error before create_linear_system");
+  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
+  EMG_CUDA(cudaSetDevice(c->device));
+  Workspace &w = *c->ws;
+  std::vector<int> slots = tidx < 0 ? std::vector<int>{EMG_SOL_MT_XY, EMG_SOL_MT_YX, EMG_SOL_DUAL}
+                                    : std::vector<int>{EMG_SOL_CSEM, EMG_SOL_DUAL};
+  int nsol = (int)slots.size();
+  const double *sp[3];
+  for (int s = 0; s < nsol; ++s) sp[s] = slot_buf(*c, slots[s]).p;
+  w.est_vol.alloc((size_t)nsol * c->nt);
+  w.est_fe.alloc((size_t)nsol * c->nt * 4);
+  w.est_eta.alloc((size_t)nsol * c->nt);
+  w.est_err.alloc((size_t)(nsol - 1) * c->nt);
+  cudaEvent_t e0, e1;
+  EMG_CUDA(cudaEventCreate(&e0));
+  EMG_CUDA(cudaEventCreate(&e1));
+  EMG_CUDA(cudaEventRecord(e0, c->stream));
+  launch_estimate(*c, 2 * PI * c->freqs[fidx], nsol, sp, w.est_eta.p, w.est_err.p, w.est_vol.p, w.est_fe.p);
+  EMG_CUDA(cudaEventRecord(e1, c->stream));
+  if (err) w.est_err.download(err, (size_t)(nsol - 1) * c->nt, c->stream);
+  if (eta_raw) w.est_eta.download(eta_raw, (size_t)nsol * c->nt, c->stream);
+  EMG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  EMG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  c->kernel_ms["estimate"] = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+// refine_fixed_fraction (src/em_fwd.cc:1182-1215)
+int emg_refine_fixed_fraction(int n, const double *err, double fraction, unsigned char *flag) {
+  EMG_API_BEGIN
+  need(n >= 0 && (n == 0 || (err && flag)), EMG_ERR_ARG, "null argument");
+  double total = 0;
+  for (int i = 0; i < n; ++i) total += err[i];
+  std::vector<double> s(err, err + n);
+  std::sort(s.begin(), s.end(), std::greater<double>());
+  double sum = 0, thr = 0;
+  for (int i = 0; i < n; ++i) {
+    if (sum < fraction * total) sum += s[i];
+    else { thr = s[i]; break; }
+  }
+  for (int i = 0; i < n; ++i)
+    if (err[i] > thr) flag[i] = 1;
+  EMG_API_END
+}
+
+// refine_fixed_number (src/em_fwd.cc:1217-1240)
+int emg_refine_fixed_number(int n, const double *err, double fraction, unsigned char *flag) {
+  EMG_API_BEGIN
+  need(n > 0 && err && flag, EMG_ERR_ARG, "null argument");
+  int k = (int)(n * fraction);
+  need(k >= 0 && k < n, EMG_ERR_ARG, "refine fraction out of range");
+  std::vector<double> s(err, err + n);
+  std::nth_element(s.begin(), s.begin() + k, s.end(), std::greater<double>());
+  double thr = s[k];
+  for (int i = 0; i < n; ++i)
+    if (err[i] > thr) flag[i] = 1;
+  EMG_API_END
+}
+
+// interpolate_fields (src/em_fwd.cc:719-744)
+int emg_interpolate_fields(emg_context *c, int target, int fidx, int n, const double *pts, const int *tets,
+                           double *eh) {
+  EMG_API_BEGIN
+  need(c && pts && tets && eh, EMG_ERR_ARG, "null argument");
+  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
+  EMG_CUDA(cudaSetDevice(c->device));
+  DBuf<double> &x = slot_buf(*c, target);
+  std::vector<double> v((size_t)c->ne * 2);
+  x.download(v.data(), v.size(), c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  typedef std::complex<double> zc;
+  const double freq = c->freqs[fidx];
+  const zc hfac = -1.0 / (zc(0, 1) * 2.0 * PI * freq * MU);
+  for (int r = 0; r < n; ++r) {
+    int t = tets[r];
+    if (t < 0 || t >= c->nt) fail(EMG_ERR_USER, "Receiver %d is not found in mesh.", r);
+    HostTet h;
+    host_tet(*c, t, h);
+    zc E[3] = {0.0, 0.0, 0.0}, H[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < 6; ++i) {
+      double phi[3];
+      int ge;
+      host_phi(*c, h, t, i, pts + 3 * r, phi, &ge);
+      int e = ge, a = c->h_edges[2 * (size_t)e], b = c->h_edges[2 * (size_t)e + 1];
+      int la = 0, lb = 0;
+      for (int q = 0; q < 4; ++q) {
+        if (h.v[q] == a) la = q;
+        if (h.v[q] == b) lb = q;
+      }
+      double cu[3] = {2.0 * (h.gr[la][1] * h.gr[lb][2] - h.gr[la][2] * h.gr[lb][1]),
+                      2.0 * (h.gr[la][2] * h.gr[lb][0] - h.gr[la][0] * h.gr[lb][2]),
+                      2.0 * (h.gr[la][0] * h.gr[lb][1] - h.gr[la][1] * h.gr[lb][0])};
+      zc u(v[2 * (size_t)e], v[2 * (size_t)e + 1]);
+      for (int d = 0; d < 3; ++d) {
+        E[d] += u * phi[d];
+        H[d] += hfac * u * cu[d];
+      }
+    }
+    for (int d = 0; d < 3; ++d) {
+      eh[12 * r + 2 * d] = E[d].real();
+      eh[12 * r + 2 * d + 1] = E[d].imag();
+      eh[12 * r + 6 + 2 * d] = H[d].real();
+      eh[12 * r + 6 + 2 * d + 1] = H[d].imag();
+    }
+  }
+  EMG_API_END
+}
+
+__global__ static void conj_copy_kernel(long n, const double2 *a, double2 *b) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) {
+    double2 v = a[i];
+    b[i] = make_double2(v.x, -v.y);
+  }
+}
+
+// batched fast path on device vectors
+static void solve_block_dev(Context &c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                            const emg_block_opts &o, emg_solve_info *infos) {
+  need(c.assembled, EMG_ERR_STATE, "solve_block before assemble_matrix");
+  need(k >= 1 && (k & (k - 1)) == 0 && k <= 32, EMG_ERR_ARG, "block width k must be a power of two <= 32");
+  Workspace &w = *c.ws;
+  const int n = c.ne;
+  std::vector<double> om(k), col(2 * k);
+  double lg = 0;
+  for (int j = 0; j < k; ++j) {
+    need(freqs[j] > 0, EMG_ERR_ARG, "frequencies must be positive");
+    om[j] = 2 * PI * freqs[j];
+    col[2 * j] = col[2 * j + 1] = om[j];
+    lg += std::log(om[j]);
+  }
+  const double wref = std::exp(lg / k);
+  const bool fp32 = o.inner_fp32 != 0;
+  if (fp32 && !w.block_ready32) {
+    ams_setup<float>(c, w.bams32, false, 0.0, wref);
+    w.block_ready32 = true;
+  }
+  if (!fp32 && !w.block_ready64) {
+    ams_setup<double>(c, w.bams64, false, 0.0, wref);
+    w.block_ready64 = true;
+  }
+  if (fp32) w.bams32.set_columns(col, c.stream);
+  else w.bams64.set_columns(col, c.stream);
+  // b = conj(s): the real-form system equals (C + i w Ms) z = conj(s)
+  w.vec_a.alloc((size_t)n * k * 2);
+  conj_copy_kernel<<<(unsigned)(((long)n * k + 255) / 256), 256, 0, c.stream>>>((long)n * k, (const double2 *)rhs_dev,
+                                                                               (double2 *)w.vec_a.p);
+  EMG_LAUNCH_CHECK();
+  w.gm.k = k;
+  w.gm.restart = o.restart > 0 ? o.restart : c.opt.gmres_restart;
+  w.gm.omega.upload(om, c.stream);
+  w.fcg64.mmax = w.fcg32.mmax = c.opt.fcg_mmax;
+  w.fcg64.verbose = w.fcg32.verbose = c.opt.verbose > 1;
+  w.fcg64.total_its = w.fcg32.total_its = 0;
+  if (fp32) {
+    w.f_in.alloc((size_t)n * k * 2);
+    w.f_out.alloc((size_t)n * k * 2);
+  }
+  // mixed precision: the AMS preconditioner (smoothers, transfers, nodal
+  // V-cycles) runs in FP32; the FCG recurrences and its operator B = C + w Ms
+  // stay in FP64, because B p loses the gradient subspace of the air in FP32
+  // (w sigma_air mu h^2 ~ 1e-10 sits far below FP32 resolution).
+  const int K2 = 2 * k;
+  if (fp32) w.omega_cols.upload(col, c.stream);
+  auto opB64 = [&](const double *p_, double *s_) {
+    SpmmArgs a;
+    a.n = n;
+    a.rp = c.rp.p;
+    a.ci = c.ci.p;
+    a.vc = c.Cv.p;
+    a.vm = c.Msv.p;
+    a.l1c = a.l1m = nullptr;
+    a.omega = w.omega_cols.p;
+    a.x = p_;
+    a.b = nullptr;
+    a.y = s_;
+    a.relax_w = 1.0;
+    a.mode = SPMM_AX;
+    spmm_nnz<double>(K2, a, c.nnz, c.stream);
+  };
+  auto pc32 = [&](const double *r_, double *z_) {
+    cvt_d2f((long)n * K2, r_, w.f_in.p, c.stream);
+    w.bams32.apply(w.f_in.p, w.f_out.p, c.stream);
+    cvt_f2d((long)n * K2, w.f_out.p, z_, c.stream);
+  };
+  auto pc = [&](const double *v, double *z) {
+    if (fp32) w.fcg64.solve_with(n, K2, pc32, opB64, v, z, c.opt.inner_rtol, c.opt.inner_max_it, c.stream);
+    else w.fcg64.solve(w.bams64, v, z, c.opt.inner_rtol, c.opt.inner_max_it, c.stream);
+  };
+  SolveStats st;
+  w.gm.solve(c, w.vec_a.p, x_dev, o.use_guess != 0, o.rtol > 0 ? o.rtol : c.opt.e_rtol,
+             o.max_it > 0 ? o.max_it : c.opt.K_max_it, false, pc, st);
+  long inner = w.fcg64.total_its;
+  if (infos)
+    for (int j = 0; j < k; ++j) fill_info(&infos[j], st, inner, j);
+  c.kernel_ms["solve_block"] = st.seconds * 1e3;
+}
+
+int emg_solve_block_dev(emg_context *c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                        const emg_block_opts *opts, emg_solve_info *infos) {
+  EMG_API_BEGIN
+  need(c && freqs && rhs_dev && x_dev && opts, EMG_ERR_ARG, "null argument");
+  EMG_CUDA(cudaSetDevice(c->device));
+  solve_block_dev(*c, k, freqs, rhs_dev, x_dev, *opts, infos);
+  EMG_API_END
+}
+
+int emg_solve_block(emg_context *c, int k, const double *freqs, const double *rhs, double *x,
+                    const emg_block_opts *opts, emg_solve_info *infos) {
+  EMG_API_BEGIN
+  need(c && freqs && rhs && x && opts, EMG_ERR_ARG, "null argument");
+  EMG_CUDA(cudaSetDevice(c->device));
+  const size_t N = (size_t)c->ne * k * 2;
+  DBuf<double> b(N), xd(N);
+  b.upload(rhs, N, c->stream);
+  if (opts->use_guess) xd.upload(x, N, c->stream);
+  solve_block_dev(*c, k, freqs, b.p, xd.p, *opts, infos);
+  xd.download(x, N, c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+int emg_spmv_complex_dev(emg_context *c, int k, const double *omegas, const double *x_dev, double *y_dev,
+                         int conj_out) {
+  EMG_API_BEGIN
+  need(c && omegas && x_dev && y_dev, EMG_ERR_ARG, "null argument");
+  need(c->assembled, EMG_ERR_STATE, "operator not assembled");
+  EMG_CUDA(cudaSetDevice(c->device));
+  c->ws->omega_k.upload(omegas, k, c->stream);
+  spmm_complex(c->ne, k, c->rp.p, c->ci.p, c->Cv.p, c->Msv.p, c->ws->omega_k.p, x_dev, nullptr, y_dev, false,
+               conj_out != 0, c->stream);
+  EMG_API_END
+}
+
+int emg_last_kernel_ms(emg_context *c, const char *name, double *ms) {
+  EMG_API_BEGIN
+  need(c && name && ms, EMG_ERR_ARG, "null argument");
+  auto it = c->kernel_ms.find(name);
+  need(it != c->kernel_ms.end(), EMG_ERR_ARG, "no timing recorded under that name");
+  *ms = it->second;
+  EMG_API_END
+}
+
+int emg_stream_synchronize(emg_context *c) {
+  EMG_API_BEGIN
+  need(c != nullptr, EMG_ERR_ARG, "null context");
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+}  // extern "C"

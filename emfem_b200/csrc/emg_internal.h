@@ -1,0 +1,204 @@
+// Internal declarations of the emfem_b200 library (host C++ + sm_100a CUDA).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/emfem_b200.h"
+
+namespace emg {
+
+constexpr double PI = 3.14159265358979323846;  // em_defs.h:16
+constexpr double MU = 4 * PI * 1E-7;           // em_defs.h:17
+constexpr double DTOR = PI / 180.0;            // em_defs.h:21
+constexpr double EPS = 1.0E-6;                 // em_defs.h:23
+
+// ---------------------------------------------------------------------------
+// errors: every C-ABI call catches Error and returns its code
+// ---------------------------------------------------------------------------
+struct Error : public std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const char *fmt, ...);
+void check_cuda(cudaError_t e, const char *what, const char *file, int line);
+#define EMG_CUDA(x) ::emg::check_cuda((x), #x, __FILE__, __LINE__)
+#define EMG_LAUNCH_CHECK() ::emg::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+
+// ---------------------------------------------------------------------------
+// device buffer (cudaMalloc-backed, move-only)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  explicit DBuf(size_t count) { alloc(count); }
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  DBuf(DBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DBuf &operator=(DBuf &&o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      (void)cudaGetLastError();
+      fail(EMG_ERR_NOMEM, "device allocation of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    }
+    n = count;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  // grows the buffer when needed (never shrinks it) and copies count elements
+  void upload(const T *h, size_t count, cudaStream_t s) {
+    if (!p || count > n) alloc(count);
+    if (count) EMG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T> &h, cudaStream_t s) { upload(h.data(), h.size(), s); }
+  void download(T *h, size_t count, cudaStream_t s) const {
+    if (count) EMG_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+  void zero(cudaStream_t s) {
+    if (n) EMG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// host CSR
+struct HCsr {
+  int n = 0, m = 0;
+  std::vector<int> rp, ci;
+  std::vector<double> vc, vm;  // two value parts (vm may be empty)
+  long nnz() const { return rp.empty() ? 0 : rp[n]; }
+};
+
+// device CSR with one or two value parts in precision T
+template <typename T>
+struct DCsr {
+  int n = 0, m = 0;
+  long nnz = 0;
+  DBuf<int> rp, ci;
+  DBuf<T> vc, vm;
+  DBuf<T> l1c, l1m;  // l1 row sums of |vc| and |vm| (smoother diagonals)
+};
+
+// ---------------------------------------------------------------------------
+// options (process_options, em_ctx.cc:100-175) + A_/B_ subset + emg keys
+// ---------------------------------------------------------------------------
+struct Options {
+  int K_max_it = 100;
+  double e_rtol = 1e-8, dual_rtol = 1e-6;
+  int inner_pc_type = 0;  // mixed=0 ams=1 direct=2
+  int pc_threshold = 500000;
+  int n_tx_divisions = 20;
+  double refine_fraction = 0.1;
+  int refine_strategy = 1;
+  int max_adaptive_refinements = 0, n_uniform_refinements = 0, max_dofs = 1000000;
+  int n_groups = 1, mesh_format = 0, direct_solver_type = 0, save_mesh = 1;
+  double max_tx_edge_length = -1, max_rx_edge_length = -1;
+  std::string iprefix, oprefix;
+  // A_ / B_ prefixes honoured by the GPU solver
+  int gmres_restart = 30;
+  double inner_rtol = 1e-2;
+  int inner_max_it = 100;
+  int fcg_mmax = 1;
+  std::string ams_cycle = "034515430";  // cycle type 13
+  int ams_relax_times = 1;
+  double ams_relax_weight = 1.0;
+  double amg_theta = 0.25;
+  int amg_pmax = 4;
+  int amg_max_coarse = 200;
+  int amg_max_levels = 25;
+  int amg_relax_times = 1;
+  // emg_*
+  int inner_fp32 = 0;
+  int graphs = 1;
+  int verbose = 0;
+};
+
+struct Workspace;
+
+// ---------------------------------------------------------------------------
+// context (mirrors EMContext, em_ctx.h:15-64)
+// ---------------------------------------------------------------------------
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Options opt;
+  // mesh
+  int nv = 0, nt = 0, ne = 0;
+  std::vector<double> h_pts;
+  std::vector<int> h_tets, h_attr, h_edges, h_t2e, h_nbr, h_non;
+  std::vector<unsigned char> h_ebdr;
+  DBuf<double> pts;
+  DBuf<int> tets, attr, edges, t2e, nbr, non;
+  DBuf<unsigned char> ebdr;
+  DBuf<int> ctet, cedge;           // canonical tets: sorted vertices, canonical edges
+  DBuf<signed char> cpar;          // parity of the vertex sort
+  // model
+  int aniso_form = 0;
+  std::vector<double> rho;
+  int nrho = 0, ncol = 0;
+  DBuf<double> sigma_tab;  // nrho x 9
+  std::vector<double> h_sigma_tab;
+  std::vector<double> freqs;
+  // background (MT boundary data)
+  std::vector<double> bg_corners, bg_ztop, bg_lsig;
+  std::vector<int> bg_nlay;
+  int bg_maxl = 0;
+  // linear system
+  bool have_ls = false;
+  int tidx = -3;
+  std::vector<int> h_rp, h_ci;
+  long nnz = 0;
+  DBuf<int> rp, ci, slot;          // slot: 36 per tet
+  DBuf<double> Cv, Msv;            // C and Ms (omega-free mass) on the pattern
+  DBuf<unsigned char> bdr_cell;
+  bool assembled = false;
+  double omega = 0;                // omega of the last assemble_matrix
+  // vertex adjacency pattern for the nodal subspace operators
+  std::vector<int> h_vrp, h_vci;
+  DBuf<int> vrp, vci, vslot;       // vslot: 16 per tet
+  DBuf<int> vinc_rp, vinc;         // vertex -> incident edge (e*2+endpoint)
+  // AMS (the preconditioner objects live in the workspace)
+  bool have_pc = false;
+  double pc_omega = 0;             // omega the hierarchy was built for (plain path)
+  // solutions: named slots, interleaved complex n
+  std::map<int, DBuf<double>> sol;
+  // timing
+  std::map<std::string, double> kernel_ms;
+  std::unique_ptr<Workspace> ws;
+  Context();
+  ~Context();
+};
+
+// helpers implemented in the .cu/.cpp files
+void sigma_table(int aniso_form, int nrho, int ncol, const double *rho, std::vector<double> &out);
+void build_sparsity(Context &c);          // host: CSR pattern (make_sparsity_patterns)
+void build_vertex_pattern(Context &c);    // host: vertex adjacency + incidence
+void canonicalize(Context &c);            // device: sorted tets + canonical edges
+void build_slot_maps(Context &c);         // device: tet -> CSR slots
+void assemble_edge(Context &c);           // device: C, Ms, bdr cells
+void assemble_nodal(Context &c, HCsr out[4]);  // device + download (G, Pi_x, Pi_y, Pi_z)
+void create_pc(Context &c, bool per_frequency_hierarchy, const std::vector<double> &omegas);
+void destroy_pc(Context &c);
+
+}  // namespace emg

@@ -1,0 +1,626 @@
+// Batched linear-algebra kernels, their launchers and the SpMM autotuner.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <sstream>
+#include <vector>
+
+#include "emg_linalg.h"
+
+namespace emg {
+
+// ---------------------------------------------------------------------------
+// SpMM dispatch and autotuning
+// ---------------------------------------------------------------------------
+using SpmmFn = void (*)(const SpmmArgs &, cudaStream_t);
+
+template <typename T, int K, int V, int NL>
+constexpr bool spmm_legal() {
+  return (K % V) == 0 && (K / V) * NL <= 32 && (32 % ((K / V) * NL)) == 0 && sizeof(T) * V <= 16;
+}
+
+template <typename T, int K, int V, int NL>
+void spmm_launch(const SpmmArgs &a, cudaStream_t s) {
+  constexpr int G = NL * (K / V);
+  constexpr int RPW = 32 / G;
+  long warps = ((long)a.n + RPW - 1) / RPW;
+  long threads = warps * 32;
+  unsigned grid = (unsigned)((threads + 255) / 256);
+  if (grid == 0) return;
+  spmm_kernel<T, K, V, NL><<<grid, 256, 0, s>>>(a);
+}
+
+template <typename T, int K, int V, int NL>
+SpmmFn spmm_pick() {
+  if constexpr (spmm_legal<T, K, V, NL>()) return &spmm_launch<T, K, V, NL>;
+  else return nullptr;
+}
+template <typename T, int K, int V>
+SpmmFn spmm_pick_nl(int nl) {
+  switch (nl) {
+  case 1: return spmm_pick<T, K, V, 1>();
+  case 2: return spmm_pick<T, K, V, 2>();
+  case 4: return spmm_pick<T, K, V, 4>();
+  case 8: return spmm_pick<T, K, V, 8>();
+  case 16: return spmm_pick<T, K, V, 16>();
+  case 32: return spmm_pick<T, K, V, 32>();
+  }
+  return nullptr;
+}
+template <typename T, int K>
+SpmmFn spmm_pick_v(int v, int nl) {
+  switch (v) {
+  case 1: return spmm_pick_nl<T, K, 1>(nl);
+  case 2: return spmm_pick_nl<T, K, 2>(nl);
+  case 4: return spmm_pick_nl<T, K, 4>(nl);
+  }
+  return nullptr;
+}
+template <typename T>
+SpmmFn spmm_fn(int K, int v, int nl) {
+  switch (K) {
+  case 1: return spmm_pick_v<T, 1>(v, nl);
+  case 2: return spmm_pick_v<T, 2>(v, nl);
+  case 4: return spmm_pick_v<T, 4>(v, nl);
+  case 8: return spmm_pick_v<T, 8>(v, nl);
+  case 16: return spmm_pick_v<T, 16>(v, nl);
+  case 32: return spmm_pick_v<T, 32>(v, nl);
+  case 64: return spmm_pick_v<T, 64>(v, nl);
+  }
+  return nullptr;
+}
+
+SpmmTuner &tuner() {
+  static SpmmTuner t;
+  return t;
+}
+
+std::string SpmmTuner::report() const {
+  std::ostringstream os;
+  for (auto &kv : best)
+    os << "T" << std::get<0>(kv.first) * 8 << " K" << std::get<1>(kv.first) << " bucket" << std::get<2>(kv.first)
+       << ": V=" << kv.second.first << " NL=" << kv.second.second << "; ";
+  return os.str();
+}
+
+static int row_bucket(const SpmmArgs &a, long nnz) {
+  double avg = a.n > 0 ? (double)nnz / a.n : 0;
+  return avg < 6 ? 0 : (avg < 12 ? 1 : (avg < 24 ? 2 : 3));
+}
+
+template <typename T>
+static std::pair<int, int> spmm_default(int K, double avg) {
+  int vmax = (int)(16 / sizeof(T));
+  int v = 1;
+  while (v * 2 <= vmax && K % (v * 2) == 0) v *= 2;
+  int cl = K / v;
+  while (cl > 32) { v *= 2; cl = K / v; }
+  int nl = 1;
+  while (nl * 2 * cl <= 32 && nl * 2 <= std::max(1.0, avg / 2)) nl *= 2;
+  return {v, nl};
+}
+
+template <typename T>
+void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
+  if (a.n <= 0) return;
+  SpmmTuner &tn = tuner();
+  int bucket = row_bucket(a, nnz);
+  auto key = std::make_tuple((int)sizeof(T), K, bucket);
+  auto it = tn.best.find(key);
+  std::pair<int, int> cfg;
+  if (it != tn.best.end()) {
+    cfg = it->second;
+  } else {
+    cfg = spmm_default<T>(K, a.n ? (double)nnz / a.n : 1.0);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    EMG_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (tn.allow_tuning && cs == cudaStreamCaptureStatusNone && a.mode != SPMM_ADD && a.n >= 20000) {
+      cudaEvent_t e0, e1;
+      EMG_CUDA(cudaEventCreate(&e0));
+      EMG_CUDA(cudaEventCreate(&e1));
+      float bestms = 1e30f;
+      for (int v : {1, 2, 4})
+        for (int nl : {1, 2, 4, 8, 16, 32}) {
+          SpmmFn f = spmm_fn<T>(K, v, nl);
+          if (!f) continue;
+          f(a, s);  // warm-up
+          EMG_CUDA(cudaEventRecord(e0, s));
+          for (int r = 0; r < 3; ++r) f(a, s);
+          EMG_CUDA(cudaEventRecord(e1, s));
+          EMG_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          EMG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < bestms) { bestms = ms; cfg = {v, nl}; }
+        }
+      EMG_CUDA(cudaEventDestroy(e0));
+      EMG_CUDA(cudaEventDestroy(e1));
+      tn.best[key] = cfg;
+      tn.tuned_count++;
+    }
+  }
+  SpmmFn f = spmm_fn<T>(K, cfg.first, cfg.second);
+  if (!f) fail(EMG_ERR_ARG, "unsupported block width K=%d", K);
+  f(a, s);
+  EMG_LAUNCH_CHECK();
+}
+
+template void spmm_nnz<float>(int, const SpmmArgs &, long, cudaStream_t);
+template void spmm_nnz<double>(int, const SpmmArgs &, long, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// column reductions and vector updates
+// ---------------------------------------------------------------------------
+static unsigned red_grid(long total) {
+  long g = (total + 255) / 256;
+  return (unsigned)std::max(1L, std::min(g, 148L * 8));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) coldot_kernel(long total, int K, const T *__restrict__ a,
+                                                     const T *__restrict__ b, double *__restrict__ out) {
+  __shared__ double sh[256];
+  double acc = 0;
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < total; i += (long)gridDim.x * 256)
+    acc += (double)a[i] * (double)b[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st >= K; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if ((int)threadIdx.x < K) atomicAdd(out + threadIdx.x, sh[threadIdx.x]);
+}
+
+template <typename T>
+void coldot(int n, int K, const T *a, const T *b, double *out, cudaStream_t s) {
+  long total = (long)n * K;
+  coldot_kernel<T><<<red_grid(total), 256, 0, s>>>(total, K, a, b, out);
+  EMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) coldot3_kernel(long total, int K, const T *__restrict__ a1,
+                                                      const T *__restrict__ b1, const T *__restrict__ a2,
+                                                      const T *__restrict__ b2, const T *__restrict__ a3,
+                                                      const T *__restrict__ b3, double *__restrict__ out) {
+  __shared__ double sh[3][256];
+  double s1 = 0, s2 = 0, s3 = 0;
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < total; i += (long)gridDim.x * 256) {
+    s1 += (double)a1[i] * (double)b1[i];
+    s2 += (double)a2[i] * (double)b2[i];
+    if (a3) s3 += (double)a3[i] * (double)b3[i];
+  }
+  sh[0][threadIdx.x] = s1;
+  sh[1][threadIdx.x] = s2;
+  sh[2][threadIdx.x] = s3;
+  __syncthreads();
+  for (int st = 128; st >= K; st >>= 1) {
+    if ((int)threadIdx.x < st) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + st];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + st];
+      sh[2][threadIdx.x] += sh[2][threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if ((int)threadIdx.x < K) {
+    atomicAdd(out + threadIdx.x, sh[0][threadIdx.x]);
+    atomicAdd(out + K + threadIdx.x, sh[1][threadIdx.x]);
+    if (a3) atomicAdd(out + 2 * K + threadIdx.x, sh[2][threadIdx.x]);
+  }
+}
+
+template <typename T>
+void coldot3(int n, int K, const T *a1, const T *b1, const T *a2, const T *b2, const T *a3, const T *b3,
+             double *out, cudaStream_t s) {
+  long total = (long)n * K;
+  coldot3_kernel<T><<<red_grid(total), 256, 0, s>>>(total, K, a1, b1, a2, b2, a3, b3, out);
+  EMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fcg_update_kernel(long total, int K, const double *__restrict__ alpha,
+                                                         const T *__restrict__ p, const T *__restrict__ sv,
+                                                         T *__restrict__ x, T *__restrict__ r,
+                                                         double *__restrict__ rn) {
+  __shared__ double sh[256];
+  double acc = 0;
+  const int c = threadIdx.x % K;
+  const double al = alpha[c];
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < total; i += (long)gridDim.x * 256) {
+    T xi = x[i] + (T)al * p[i];
+    T ri = r[i] - (T)al * sv[i];
+    x[i] = xi;
+    r[i] = ri;
+    acc += (double)ri * (double)ri;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st >= K; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if ((int)threadIdx.x < K) atomicAdd(rn + threadIdx.x, sh[threadIdx.x]);
+}
+
+template <typename T>
+void fcg_update(int n, int K, const double *alpha, const T *p, const T *sv, T *x, T *r, double *rn,
+                cudaStream_t s) {
+  long total = (long)n * K;
+  fcg_update_kernel<T><<<red_grid(total), 256, 0, s>>>(total, K, alpha, p, sv, x, r, rn);
+  EMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+__global__ void fcg_direction_kernel(long total, int K, const T *__restrict__ z, int nprev, T *const *Pj,
+                                     const double *__restrict__ beta, T *__restrict__ p) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int c = (int)(i % K);
+  double v = (double)z[i];
+  for (int j = 0; j < nprev; ++j) v -= beta[j * K + c] * (double)Pj[j][i];
+  p[i] = (T)v;
+}
+
+template <typename T>
+void fcg_direction(int n, int K, const T *z, int nprev, T *const *Pj, const double *beta, T *p, cudaStream_t st) {
+  long total = (long)n * K;
+  fcg_direction_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(total, K, z, nprev, Pj, beta, p);
+  EMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+__global__ void jacobi0_kernel(long total, int K, const T *__restrict__ b, const T *__restrict__ l1c,
+                               const T *__restrict__ l1m, const double *__restrict__ omega, double w,
+                               T *__restrict__ y) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  long row = i / K;
+  int c = (int)(i % K);
+  T d = l1c[row];
+  if (l1m) d += (T)omega[c] * l1m[row];
+  y[i] = (T)w * b[i] / d;
+}
+
+template <typename T>
+void jacobi0(int n, int K, const T *b, const T *l1c, const T *l1m, const double *omega, double w, T *y,
+             cudaStream_t s) {
+  long total = (long)n * K;
+  if (!total) return;
+  jacobi0_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, b, l1c, l1m, omega, w, y);
+  EMG_LAUNCH_CHECK();
+}
+
+__global__ void cvt_d2f_kernel(long n, const double *__restrict__ a, float *__restrict__ b) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+__global__ void cvt_f2d_kernel(long n, const float *__restrict__ a, double *__restrict__ b) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+void cvt_d2f(long count, const double *a, float *b, cudaStream_t s) {
+  if (!count) return;
+  cvt_d2f_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(count, a, b);
+  EMG_LAUNCH_CHECK();
+}
+void cvt_f2d(long count, const float *a, double *b, cudaStream_t s) {
+  if (!count) return;
+  cvt_f2d_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(count, a, b);
+  EMG_LAUNCH_CHECK();
+}
+template <typename T>
+void fill_zero(long count, T *a, cudaStream_t s) {
+  if (count) EMG_CUDA(cudaMemsetAsync(a, 0, count * sizeof(T), s));
+}
+
+// ---------------------------------------------------------------------------
+// AMS transfers
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void ams_restrict_kernel(int nv, int K, int sp, const int *__restrict__ inc_rp,
+                                    const int *__restrict__ inc, const T *__restrict__ tangent,
+                                    const T *__restrict__ r_edge, T *__restrict__ r_vert) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)nv * K) return;
+  int v = (int)(i / K), c = (int)(i % K);
+  T acc = 0;
+  const int kb = __ldg(inc_rp + v), ke = __ldg(inc_rp + v + 1);
+  for (int k = kb; k < ke; ++k) {
+    int code = __ldg(inc + k);
+    int e = code >> 1;
+    T w;
+    if (sp == 0) w = (code & 1) ? T(1) : T(-1);
+    else w = T(0.5) * __ldg(tangent + 3 * (long)e + (sp - 1));
+    acc += w * __ldg(r_edge + (long)e * K + c);
+  }
+  r_vert[i] = acc;
+}
+
+template <typename T>
+void ams_restrict(int nv, int K, int sp, const int *inc_rp, const int *inc, const T *tangent, const T *r_edge,
+                  T *r_vert, cudaStream_t s) {
+  long total = (long)nv * K;
+  ams_restrict_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(nv, K, sp, inc_rp, inc, tangent, r_edge,
+                                                                         r_vert);
+  EMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+__global__ void ams_prolong_kernel(int ne, int K, int sp, const int *__restrict__ edges,
+                                   const T *__restrict__ tangent, const T *__restrict__ ev, T *__restrict__ x) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)ne * K) return;
+  int e = (int)(i / K), c = (int)(i % K);
+  int v0 = __ldg(edges + 2 * (long)e), v1 = __ldg(edges + 2 * (long)e + 1);
+  T a = __ldg(ev + (long)v0 * K + c), b = __ldg(ev + (long)v1 * K + c);
+  T val;
+  if (sp == 0) val = b - a;
+  else val = T(0.5) * __ldg(tangent + 3 * (long)e + (sp - 1)) * (a + b);
+  x[i] += val;
+}
+
+template <typename T>
+void ams_prolong_add(int ne, int K, int sp, const int *edges, const T *tangent, const T *e_vert, T *x_edge,
+                     cudaStream_t s) {
+  long total = (long)ne * K;
+  ams_prolong_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(ne, K, sp, edges, tangent, e_vert, x_edge);
+  EMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+__global__ void coarse_apply_kernel(int nc, int K, const double *__restrict__ inv, const int *__restrict__ slot,
+                                    const T *__restrict__ b, T *__restrict__ x) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)nc * K) return;
+  int r = (int)(i / K), c = (int)(i % K);
+  const double *row = inv + ((long)__ldg(slot + c) * nc + r) * nc;
+  double acc = 0;
+  for (int j = 0; j < nc; ++j) acc += __ldg(row + j) * (double)b[(long)j * K + c];
+  x[i] = (T)acc;
+}
+
+template <typename T>
+void coarse_apply(int nc, int K, const double *inv, const int *col_slot, const T *b, T *x, cudaStream_t s) {
+  long total = (long)nc * K;
+  if (!total) return;
+  coarse_apply_kernel<T><<<(unsigned)((total + 127) / 128), 128, 0, s>>>(nc, K, inv, col_slot, b, x);
+  EMG_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// complex FP64 kernels of the outer FGMRES
+// ---------------------------------------------------------------------------
+template <int K, int NL>
+__global__ void __launch_bounds__(256) spmm_complex_kernel(int n, const int *__restrict__ rp,
+                                                           const int *__restrict__ ci, const double *__restrict__ Cv,
+                                                           const double *__restrict__ Mv,
+                                                           const double *__restrict__ omega,
+                                                           const double2 *__restrict__ x,
+                                                           const double2 *__restrict__ b, double2 *__restrict__ y,
+                                                           bool residual, bool conj_out) {
+  constexpr int G = K * NL;
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int row = gwarp * (32 / G) + lane / G;
+  const int sub = lane % G;
+  const int c = sub % K, sl = sub / K;
+  const double w = __ldg(omega + c);
+  double ar = 0, ai = 0;
+  const bool valid = row < n;
+  if (valid) {
+    const int kb = __ldg(rp + row), ke = __ldg(rp + row + 1);
+    for (int k = kb + sl; k < ke; k += NL) {
+      const int j = __ldg(ci + k);
+      const double a = __ldg(Cv + k), m = w * __ldg(Mv + k);
+      const double2 xv = __ldg(x + (long)j * K + c);
+      ar = fma(a, xv.x, fma(-m, xv.y, ar));
+      ai = fma(a, xv.y, fma(m, xv.x, ai));
+    }
+  }
+#pragma unroll
+  for (int off = K; off < G; off <<= 1) {
+    ar += __shfl_xor_sync(0xffffffffu, ar, off);
+    ai += __shfl_xor_sync(0xffffffffu, ai, off);
+  }
+  if (!valid || sl != 0) return;
+  if (conj_out) ai = -ai;
+  const long o = (long)row * K + c;
+  if (residual) {
+    double2 bv = __ldg(b + o);
+    y[o] = make_double2(bv.x - ar, bv.y - ai);
+  } else {
+    y[o] = make_double2(ar, ai);
+  }
+}
+
+template <int K>
+static void spmm_complex_k(int n, const int *rp, const int *ci, const double *Cv, const double *Mv,
+                           const double *omega, const double *x, const double *b, double *y, bool residual,
+                           bool conj_out, cudaStream_t s) {
+  constexpr int NL = (32 / K) >= 8 ? 8 : (32 / K);
+  constexpr int RPW = 32 / (K * NL);
+  long warps = ((long)n + RPW - 1) / RPW;
+  unsigned grid = (unsigned)((warps * 32 + 255) / 256);
+  spmm_complex_kernel<K, NL><<<grid, 256, 0, s>>>(n, rp, ci, Cv, Mv, omega, (const double2 *)x, (const double2 *)b,
+                                                  (double2 *)y, residual, conj_out);
+  EMG_LAUNCH_CHECK();
+}
+
+void spmm_complex(int n, int K, const int *rp, const int *ci, const double *Cv, const double *Mv,
+                  const double *omega, const double *x, const double *b, double *y, bool residual, bool conj_out,
+                  cudaStream_t s) {
+  switch (K) {
+  case 1: return spmm_complex_k<1>(n, rp, ci, Cv, Mv, omega, x, b, y, residual, conj_out, s);
+  case 2: return spmm_complex_k<2>(n, rp, ci, Cv, Mv, omega, x, b, y, residual, conj_out, s);
+  case 4: return spmm_complex_k<4>(n, rp, ci, Cv, Mv, omega, x, b, y, residual, conj_out, s);
+  case 8: return spmm_complex_k<8>(n, rp, ci, Cv, Mv, omega, x, b, y, residual, conj_out, s);
+  case 16: return spmm_complex_k<16>(n, rp, ci, Cv, Mv, omega, x, b, y, residual, conj_out, s);
+  case 32: return spmm_complex_k<32>(n, rp, ci, Cv, Mv, omega, x, b, y, residual, conj_out, s);
+  }
+  fail(EMG_ERR_ARG, "unsupported complex block width %d", K);
+}
+
+constexpr int MAXJ = 32;
+
+__global__ void __launch_bounds__(256) cmultidot_kernel(long total, int K, int J, const double2 *__restrict__ V,
+                                                        long stride, const double2 *__restrict__ w,
+                                                        double *__restrict__ h) {
+  double hr[MAXJ], hi[MAXJ];
+#pragma unroll
+  for (int j = 0; j < MAXJ; ++j) { hr[j] = 0; hi[j] = 0; }
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < total; i += (long)gridDim.x * 256) {
+    double2 wv = w[i];
+#pragma unroll
+    for (int j = 0; j < MAXJ; ++j) {
+      if (j < J) {
+        double2 v = __ldg(V + j * stride + i);
+        hr[j] = fma(v.x, wv.x, fma(v.y, wv.y, hr[j]));
+        hi[j] = fma(v.x, wv.y, fma(-v.y, wv.x, hi[j]));
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < MAXJ; ++j) {
+    if (j < J) {
+      double a = hr[j], b = hi[j];
+      for (int off = K; off < 32; off <<= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+      }
+      if (lane < K) {
+        atomicAdd(h + 2 * (j * K + lane), a);
+        atomicAdd(h + 2 * (j * K + lane) + 1, b);
+      }
+    }
+  }
+}
+
+void cmultidot(int n, int K, int J, const double *V, long stride, const double *w, double *h, double *partial,
+               int partial_blocks, cudaStream_t s) {
+  (void)partial;
+  (void)partial_blocks;
+  if (J > MAXJ) fail(EMG_ERR_ARG, "restart above %d", MAXJ);
+  if (K > 32) fail(EMG_ERR_ARG, "complex block width above 32");
+  EMG_CUDA(cudaMemsetAsync(h, 0, sizeof(double) * 2 * J * K, s));
+  long total = (long)n * K;
+  unsigned grid = (unsigned)std::max(1L, std::min((total + 255) / 256, 148L * 2));
+  cmultidot_kernel<<<grid, 256, 0, s>>>(total, K, J, (const double2 *)V, stride / 2, (const double2 *)w, h);
+  EMG_LAUNCH_CHECK();
+}
+
+__global__ void __launch_bounds__(256) cgs_update_kernel(long total, int K, int J, const double2 *__restrict__ V,
+                                                         long stride, const double *__restrict__ h,
+                                                         double2 *__restrict__ w, double *__restrict__ hn) {
+  __shared__ double sh[256];
+  double acc = 0;
+  const int c = threadIdx.x % K;
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < total; i += (long)gridDim.x * 256) {
+    double2 wv = w[i];
+    for (int j = 0; j < J; ++j) {
+      double2 v = __ldg(V + j * stride + i);
+      double a = h[2 * (j * K + c)], b = h[2 * (j * K + c) + 1];
+      wv.x -= a * v.x - b * v.y;
+      wv.y -= a * v.y + b * v.x;
+    }
+    w[i] = wv;
+    acc += wv.x * wv.x + wv.y * wv.y;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st >= K; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if ((int)threadIdx.x < K) atomicAdd(hn + threadIdx.x, sh[threadIdx.x]);
+}
+
+void cgs_update(int n, int K, int J, const double *V, long stride, const double *h, double *w, double *hn,
+                cudaStream_t s) {
+  EMG_CUDA(cudaMemsetAsync(hn, 0, sizeof(double) * K, s));
+  long total = (long)n * K;
+  cgs_update_kernel<<<red_grid(total), 256, 0, s>>>(total, K, J, (const double2 *)V, stride / 2, h, (double2 *)w,
+                                                    hn);
+  EMG_LAUNCH_CHECK();
+}
+
+__global__ void cscale_kernel(long total, int K, const double2 *__restrict__ w, const double *__restrict__ sc,
+                              double2 *__restrict__ v) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  double f = sc[i % K];
+  f = f > 0 ? 1.0 / f : 0.0;
+  double2 a = w[i];
+  v[i] = make_double2(a.x * f, a.y * f);
+}
+
+void cscale(int n, int K, const double *w, const double *scale, double *v, cudaStream_t s) {
+  long total = (long)n * K;
+  cscale_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, (const double2 *)w, scale, (double2 *)v);
+  EMG_LAUNCH_CHECK();
+}
+
+__global__ void cupdate_kernel(long total, int K, int J, const double2 *__restrict__ Z, long stride,
+                               const double *__restrict__ y, double2 *__restrict__ x) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int c = (int)(i % K);
+  double2 xv = x[i];
+  for (int j = 0; j < J; ++j) {
+    double2 z = __ldg(Z + j * stride + i);
+    double a = y[2 * (j * K + c)], b = y[2 * (j * K + c) + 1];
+    xv.x += a * z.x - b * z.y;
+    xv.y += a * z.y + b * z.x;
+  }
+  x[i] = xv;
+}
+
+void cupdate(int n, int K, int J, const double *Z, long stride, const double *y, double *x, cudaStream_t s) {
+  long total = (long)n * K;
+  cupdate_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, J, (const double2 *)Z, stride / 2, y,
+                                                                 (double2 *)x);
+  EMG_LAUNCH_CHECK();
+}
+
+__global__ void __launch_bounds__(256) cnorm2_kernel(long total, int K, const double2 *__restrict__ x,
+                                                     double *__restrict__ out) {
+  __shared__ double sh[256];
+  double acc = 0;
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < total; i += (long)gridDim.x * 256) {
+    double2 v = x[i];
+    acc += v.x * v.x + v.y * v.y;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st >= K; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if ((int)threadIdx.x < K) atomicAdd(out + threadIdx.x, sh[threadIdx.x]);
+}
+
+void cnorm2(int n, int K, const double *x, double *out, cudaStream_t s) {
+  long total = (long)n * K;
+  cnorm2_kernel<<<red_grid(total), 256, 0, s>>>(total, K, (const double2 *)x, out);
+  EMG_LAUNCH_CHECK();
+}
+
+// explicit instantiations
+#define EMG_INST(T)                                                                                              \
+  template void coldot<T>(int, int, const T *, const T *, double *, cudaStream_t);                              \
+  template void coldot3<T>(int, int, const T *, const T *, const T *, const T *, const T *, const T *, double *,  \
+                           cudaStream_t);                                                                        \
+  template void fcg_update<T>(int, int, const double *, const T *, const T *, T *, T *, double *, cudaStream_t); \
+  template void fcg_direction<T>(int, int, const T *, int, T *const *, const double *, T *, cudaStream_t);       \
+  template void jacobi0<T>(int, int, const T *, const T *, const T *, const double *, double, T *, cudaStream_t); \
+  template void fill_zero<T>(long, T *, cudaStream_t);                                                           \
+  template void ams_restrict<T>(int, int, int, const int *, const int *, const T *, const T *, T *, cudaStream_t); \
+  template void ams_prolong_add<T>(int, int, int, const int *, const T *, const T *, T *, cudaStream_t);          \
+  template void coarse_apply<T>(int, int, const double *, const int *, const T *, T *, cudaStream_t);
+EMG_INST(float)
+EMG_INST(double)
+#undef EMG_INST
+
+}  // namespace emg

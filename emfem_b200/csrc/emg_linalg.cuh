@@ -1,0 +1,168 @@
+// Batched sparse kernels over block vectors.
+//
+// Block vectors are n x K row-major (the K columns of a row are contiguous),
+// so one pass over a matrix row serves every column.  Operators are stored as
+// one CSR pattern with one or two value parts: A(w_c) = Ac + w_c * Am, where
+// w_c is the angular frequency of column c.  This is the form of every
+// operator of the path: B = C + w Ms on edges (src/em_la.cc:122-128) and the
+// Galerkin operators of the nodal AMS subspaces, which are affine in w once
+// their interpolation is fixed.
+//
+// Lane layout of spmm_kernel<T, K, V, NL>: a row is served by NL*CL lanes,
+// CL = K/V lanes over column blocks of V contiguous columns (vector loads of
+// V*sizeof(T) bytes) and NL lanes splitting the row's nonzeros (reduced with
+// warp shuffles); 32/(NL*CL) rows per warp.  (V, NL) per (T, K) is picked by
+// the autotuner in emg_linalg.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace emg {
+
+enum SpmmMode : int {
+  SPMM_AX = 0,    // y = A x
+  SPMM_RES = 1,   // y = b - A x
+  SPMM_JAC = 2,   // y = x + w (b - A x) / d,  d = l1c + w_c l1m
+  SPMM_ADD = 3,   // y = y + A x   (prolongation)
+};
+
+template <typename T, int V>
+struct VecT;
+template <> struct VecT<float, 1> { typedef float type; };
+template <> struct VecT<float, 2> { typedef float2 type; };
+template <> struct VecT<float, 4> { typedef float4 type; };
+template <> struct VecT<double, 1> { typedef double type; };
+template <> struct VecT<double, 2> { typedef double2 type; };
+
+template <typename T, int V>
+__device__ __forceinline__ void ldv(const T *__restrict__ p, T (&v)[V]) {
+  typedef typename VecT<T, V>::type VT;
+  VT t = __ldg(reinterpret_cast<const VT *>(p));
+  const T *s = reinterpret_cast<const T *>(&t);
+#pragma unroll
+  for (int i = 0; i < V; ++i) v[i] = s[i];
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void ldv_plain(const T *p, T (&v)[V]) {
+  typedef typename VecT<T, V>::type VT;
+  VT t = *reinterpret_cast<const VT *>(p);
+  const T *s = reinterpret_cast<const T *>(&t);
+#pragma unroll
+  for (int i = 0; i < V; ++i) v[i] = s[i];
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void stv(T *p, const T (&v)[V]) {
+  typedef typename VecT<T, V>::type VT;
+  VT t;
+  T *s = reinterpret_cast<T *>(&t);
+#pragma unroll
+  for (int i = 0; i < V; ++i) s[i] = v[i];
+  *reinterpret_cast<VT *>(p) = t;
+}
+
+struct SpmmArgs {
+  int n;
+  const int *rp, *ci;
+  const void *vc, *vm;     // value parts (vm may be null)
+  const void *l1c, *l1m;   // l1 row sums for SPMM_JAC
+  const double *omega;     // K per-column shifts (device), may be null if vm null
+  const void *x, *b;
+  void *y;
+  double relax_w;
+  int mode;
+};
+
+template <typename T, int K, int V, int NL>
+__global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
+  constexpr int CL = K / V;
+  constexpr int G = NL * CL;
+  static_assert(G <= 32 && (32 % G) == 0, "bad lane layout");
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int row = gwarp * (32 / G) + lane / G;
+  const int sub = lane % G;
+  const int cb = sub % CL;      // column block
+  const int sl = sub / CL;      // nonzero slice
+  const T *__restrict__ vc = static_cast<const T *>(a.vc);
+  const T *__restrict__ vm = static_cast<const T *>(a.vm);
+  const T *__restrict__ x = static_cast<const T *>(a.x);
+  T acc[V];
+#pragma unroll
+  for (int i = 0; i < V; ++i) acc[i] = T(0);
+  T w[V];
+  const bool two = vm != nullptr;
+  if (two) {
+#pragma unroll
+    for (int i = 0; i < V; ++i) w[i] = (T)__ldg(a.omega + cb * V + i);
+  }
+  const bool valid = row < a.n;
+  if (valid) {
+    const int kb = __ldg(a.rp + row), ke = __ldg(a.rp + row + 1);
+    if (two) {
+      for (int k = kb + sl; k < ke; k += NL) {
+        const int j = __ldg(a.ci + k);
+        const T c = __ldg(vc + k), m = __ldg(vm + k);
+        T xv[V];
+        ldv<T, V>(x + (long)j * K + cb * V, xv);
+#pragma unroll
+        for (int i = 0; i < V; ++i) acc[i] = fma(c + w[i] * m, xv[i], acc[i]);
+      }
+    } else {
+      for (int k = kb + sl; k < ke; k += NL) {
+        const int j = __ldg(a.ci + k);
+        const T c = __ldg(vc + k);
+        T xv[V];
+        ldv<T, V>(x + (long)j * K + cb * V, xv);
+#pragma unroll
+        for (int i = 0; i < V; ++i) acc[i] = fma(c, xv[i], acc[i]);
+      }
+    }
+  }
+#pragma unroll
+  for (int off = CL; off < G; off <<= 1)
+#pragma unroll
+    for (int i = 0; i < V; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+  if (!valid || sl != 0) return;
+  const long o = (long)row * K + cb * V;
+  T *y = static_cast<T *>(a.y);
+  T out[V];
+  switch (a.mode) {
+  case SPMM_AX:
+#pragma unroll
+    for (int i = 0; i < V; ++i) out[i] = acc[i];
+    break;
+  case SPMM_RES: {
+    T bv[V];
+    ldv<T, V>(static_cast<const T *>(a.b) + o, bv);
+#pragma unroll
+    for (int i = 0; i < V; ++i) out[i] = bv[i] - acc[i];
+    break;
+  }
+  case SPMM_JAC: {
+    T bv[V], xo[V];
+    ldv<T, V>(static_cast<const T *>(a.b) + o, bv);
+    ldv<T, V>(x + o, xo);
+    const T dc = __ldg(static_cast<const T *>(a.l1c) + row);
+    const T dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      T d = two ? dc + w[i] * dm : dc;
+      out[i] = xo[i] + (T)a.relax_w * (bv[i] - acc[i]) / d;
+    }
+    break;
+  }
+  default: {  // SPMM_ADD
+    T yo[V];
+    ldv_plain<T, V>(y + o, yo);
+#pragma unroll
+    for (int i = 0; i < V; ++i) out[i] = yo[i] + acc[i];
+  }
+  }
+  stv<T, V>(y + o, out);
+}
+
+}  // namespace emg

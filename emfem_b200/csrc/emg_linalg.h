@@ -1,0 +1,86 @@
+// Host interface of the batched linear-algebra kernels (emg_linalg.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+
+#include "emg_internal.h"
+#include "emg_linalg.cuh"
+
+namespace emg {
+
+// SpMM launcher with an autotuned lane layout per (precision, K, row-length
+// class).  Tuning runs on the first large non-accumulating call it sees and
+// times every legal (V, NL) candidate with CUDA events.
+struct SpmmTuner {
+  std::map<std::tuple<int, int, int>, std::pair<int, int>> best;  // (sizeof T, K, bucket) -> (V, NL)
+  bool allow_tuning = true;
+  int tuned_count = 0;
+  std::string report() const;
+};
+
+SpmmTuner &tuner();
+
+// nnz of the operator selects the row-length class of the tuning table
+template <typename T>
+void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s);
+
+// out[c] (+)= sum_i a[i*K+c] * b[i*K+c]   (FP64 accumulation); out must be zeroed
+template <typename T>
+void coldot(int n, int K, const T *a, const T *b, double *out, cudaStream_t s);
+// three dot products in one pass: out[0..K) = (a1,b1), out[K..2K) = (a2,b2), out[2K..3K) = (a3,b3)
+template <typename T>
+void coldot3(int n, int K, const T *a1, const T *b1, const T *a2, const T *b2, const T *a3, const T *b3,
+             double *out, cudaStream_t s);
+// x += alpha_c p ; r -= alpha_c s ; rn[c] += ||r_c||^2
+template <typename T>
+void fcg_update(int n, int K, const double *alpha, const T *p, const T *sv, T *x, T *r, double *rn, cudaStream_t s);
+// p = z - sum_j beta[j*K+c] * P_j  (nprev directions, pointers in a device array)
+template <typename T>
+void fcg_direction(int n, int K, const T *z, int nprev, T *const *Pj, const double *beta, T *p, cudaStream_t st);
+// y = w * b / d   (first l1-Jacobi sweep from a zero guess)
+template <typename T>
+void jacobi0(int n, int K, const T *b, const T *l1c, const T *l1m, const double *omega, double w, T *y,
+             cudaStream_t s);
+// precision conversion of block vectors
+void cvt_d2f(long count, const double *a, float *b, cudaStream_t s);
+void cvt_f2d(long count, const float *a, double *b, cudaStream_t s);
+template <typename T>
+void fill_zero(long count, T *a, cudaStream_t s);
+
+// AMS transfers between edges and vertices for K columns.
+//   sp == 0: gradient G (row e: -1 at edges[e][0], +1 at edges[e][1])
+//   sp == 1..3: Pi_d, d = sp-1 (row e: 0.5 t_e[d] at both endpoints)
+template <typename T>
+void ams_restrict(int nv, int K, int sp, const int *inc_rp, const int *inc, const T *tangent, const T *r_edge,
+                  T *r_vert, cudaStream_t s);
+template <typename T>
+void ams_prolong_add(int ne, int K, int sp, const int *edges, const T *tangent, const T *e_vert, T *x_edge,
+                     cudaStream_t s);
+// x[i,c] = sum_j inv[slot(c)][i][j] b[j,c]  (FP64 generalized inverse of the coarsest operator)
+template <typename T>
+void coarse_apply(int nc, int K, const double *inv, const int *col_slot, const T *b, T *x, cudaStream_t s);
+
+// ---- complex (FP64) kernels of the outer FGMRES ------------------------------
+// y = b - A(w_c) x  or  y = A(w_c) x, complex n x K; conj_out conjugates the
+// product (the real-form operator of matshell_mult_a).
+void spmm_complex(int n, int K, const int *rp, const int *ci, const double *Cv, const double *Mv,
+                  const double *omega, const double *x, const double *b, double *y, bool residual, bool conj_out,
+                  cudaStream_t s);
+// h[j*K+c] = sum_i conj(V_j[i,c]) w[i,c]  for j < J (complex), V_j = V + j*stride
+void cmultidot(int n, int K, int J, const double *V, long stride, const double *w, double *h, double *partial,
+               int partial_blocks, cudaStream_t s);
+// w -= sum_j h[j*K+c] V_j ; hn[c] = ||w_c||^2
+void cgs_update(int n, int K, int J, const double *V, long stride, const double *h, double *w, double *hn,
+                cudaStream_t s);
+// v = w / scale[c]  (scale real)
+void cscale(int n, int K, const double *w, const double *scale, double *v, cudaStream_t s);
+// x += sum_j y[j*K+c] Z_j   (complex coefficients)
+void cupdate(int n, int K, int J, const double *Z, long stride, const double *y, double *x, cudaStream_t s);
+// out[c] += ||x_c||^2 over complex columns
+void cnorm2(int n, int K, const double *x, double *out, cudaStream_t s);
+
+}  // namespace emg

@@ -1,0 +1,191 @@
+/*
+ * emfem_b200 -- C ABI of the B200-native EMFEM forward-solve path.
+ *
+ * One opaque context mirrors the reference's EMContext (src/em_ctx.h:15-64):
+ * it owns the mesh arrays, the assembled operators, the AMS preconditioner and
+ * the named solution vectors, all resident in the device memory of one GPU.
+ * Every entry point returns 0 on success or a negative status; the message
+ * of the last failure on the calling thread is available from
+ * emg_last_error().  Vectors cross the boundary as plain host pointers (the
+ * *_dev variants take device pointers); nothing in this header uses torch
+ * or PETSc types.  Single-threaded per context, like the reference.
+ */
+#ifndef EMFEM_B200_H
+#define EMFEM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define EMG_OK 0
+#define EMG_ERR_USER (-1)          /* EM_ERR_USER, src/em_defs.h:76            */
+#define EMG_ERR_ARG (-2)           /* bad argument (null pointer, size)       */
+#define EMG_ERR_STATE (-3)         /* call out of order (e.g. solve before pc) */
+#define EMG_ERR_CUDA (-4)          /* CUDA runtime error                       */
+#define EMG_ERR_NOMEM (-5)         /* device allocation failed                 */
+#define EMG_DIVERGED_ITS (-6)      /* Krylov hit max_it before rtol            */
+#define EMG_DIVERGED_NANORINF (-7) /* NaN or Inf in a residual                 */
+#define EMG_ERR_OPTION (-8)        /* unknown or malformed option              */
+
+/* anisotropy forms, src/em_defs.h:37 */
+#define EMG_ISOTROPIC 0
+#define EMG_VERTICAL 1
+#define EMG_TRIAXIAL 2
+#define EMG_ARBITRARY 3
+
+/* named solution slots: ctx->mt_e[XY_POLAR], mt_e[YX_POLAR], csem_e, dual_e
+ * (src/em_ctx.h:44-45, src/em_defs.h:39) */
+#define EMG_SOL_MT_XY (-1)
+#define EMG_SOL_MT_YX (-2)
+#define EMG_SOL_CSEM 0
+#define EMG_SOL_DUAL 1
+
+typedef struct emg_context emg_context;
+
+typedef struct emg_solve_info {
+  int outer_its;        /* FGMRES iterations                                 */
+  int inner_its;        /* total FCG iterations (both real blocks)           */
+  int reason;           /* 0 converged, EMG_DIVERGED_* otherwise             */
+  double true_rel_res;  /* ||b - A x|| / ||b|| recomputed in FP64 at exit    */
+  double seconds;       /* device time of the solve                          */
+} emg_solve_info;
+
+const char *emg_last_error(void);
+const char *emg_version(void);
+
+/* create_context / destroy_context (src/em_ctx.cc:7-98). device: CUDA ordinal. */
+int emg_create_context(emg_context **ctx, int device);
+int emg_destroy_context(emg_context *ctx);
+
+/* process_options (src/em_ctx.cc:100-175): PETSc options-file text ("-key
+ * value" tokens, '#' comments).  Honours -K_max_it -e_rtol -dual_rtol
+ * -inner_pc_type -pc_threshold -n_tx_divisions -refine_fraction
+ * -refine_strategy -max_adaptive_refinements -n_uniform_refinements
+ * -max_dofs -save_mesh -iprefix -oprefix -n_groups -max_tx_edge_length
+ * -max_rx_edge_length -mesh_format -direct_solver_type, the A_/B_ subset the
+ * GPU solver implements (A_ksp_gmres_restart, B_ksp_rtol, B_ksp_max_it,
+ * B_pc_hypre_ams_cycle_type, B_pc_hypre_ams_relax_times, ...) and the
+ * -emg_* keys of this implementation.  Unknown keys: EMG_ERR_OPTION. */
+int emg_process_options(emg_context *ctx, const char *options_text);
+int emg_get_option(emg_context *ctx, const char *key, double *value);
+
+/* Mesh arrays as the host Mesh keeps them (src/em_mesh.h:81-96, one rank:
+ * identity numbering).  Copied to the device; edge numbering is never
+ * changed.  edge_bdr: edge_bdr_marker_ (src/em_mesh.cc:483-502). */
+int emg_set_mesh(emg_context *ctx, int n_vertices, const double *pointlist, int n_tets,
+                 const int *tetrahedronlist, const int *attributes, int n_edges, const int *edgelist,
+                 const int *tet2edgelist, const int *neighborlist, const int *tet_non,
+                 const unsigned char *edge_bdr_marker);
+
+/* read_rho (src/em_io.cc:9-86): n_rho rows of ncol resistivities (and
+ * Euler angles in degrees for the Arbitrary form). */
+int emg_set_model(emg_context *ctx, int aniso_form, int n_rho, int ncol, const double *rho);
+
+/* ctx->freqs (src/em_ctx.h:21) */
+int emg_set_frequencies(emg_context *ctx, int n, const double *freqs);
+
+/* create_linear_system / destroy_linear_system (src/em_fwd.cc:248-316).
+ * tidx < 0: MT (two primal slots), tidx >= 0: CSEM. */
+int emg_create_linear_system(emg_context *ctx, int tidx);
+int emg_destroy_linear_system(emg_context *ctx);
+
+/* make_sparsity_patterns (src/em_fwd.cc:191-246): *nnz always set; rptr
+ * (n_edges+1) and cidx (nnz) filled when non-null. */
+int emg_get_sparsity(emg_context *ctx, long *nnz, int *rptr, int *cidx);
+
+/* assemble_matrix (src/em_fwd.cc:318-400) for frequency ctx->freqs[fidx]:
+ * C (curl-curl/mu) and M (omega * mass) on the shared pattern, boundary
+ * rows/columns zeroed as the reference does.  Values stay on the device;
+ * emg_get_matrices copies them out (either pointer may be null), bdr_cells
+ * (n_tets flags) is the reference's ctx->bdr_cells set. */
+int emg_assemble_matrix(emg_context *ctx, int fidx);
+int emg_get_matrices(emg_context *ctx, double *C, double *M, unsigned char *bdr_cells);
+
+/* create_pc / destroy_pc (src/em_la.cc:113-206) incl. setup_ams
+ * (src/em_la.cc:230-295): B = C + M and the AMS hierarchy. */
+int emg_create_pc(emg_context *ctx);
+int emg_destroy_pc(emg_context *ctx);
+
+/* matshell_mult_a (src/em_la.cc:65-87) on host vectors of length 2n
+ * ([re block; im block], the VecNest layout): y = [C xr - M xi; -M xr - C xi]. */
+int emg_matshell_mult_a(emg_context *ctx, const double *x, double *y);
+
+/* pc_apply_b (src/em_la.cc:208-228): x = [B^-1 br; B^-1 bi], each an FCG(AMS)
+ * solve to the inner tolerance. */
+int emg_pc_apply_b(emg_context *ctx, const double *b, double *x);
+
+/* solve_linear_system (src/em_la.cc:35-63): real-form FGMRES right-
+ * preconditioned by pc_apply_b, zero initial guess, into named slot
+ * `target` (EMG_SOL_*).  Returns EMG_DIVERGED_ITS if max_it is hit (the
+ * reference is silent there) -- the slot still holds the last iterate. */
+int emg_solve_linear_system(emg_context *ctx, int target, const double *s_re, const double *s_im,
+                            int max_it, double rtol, emg_solve_info *info);
+
+/* access_vec / VecGetArray on a named slot (src/em_la.cc:7-33). */
+int emg_get_solution(emg_context *ctx, int target, double *e_re, double *e_im);
+int emg_set_solution(emg_context *ctx, int target, const double *e_re, const double *e_im);
+
+/* RHS assembly (src/em_fwd.cc:402-717) into host vectors s_re/s_im.
+ * MT: needs the layered background columns under the four top corners
+ * (update_background_model, src/em_fwd.cc:135-159): corners 4x3, nlay[4],
+ * ztop/lsig laid out 4 x maxl. */
+int emg_set_background(emg_context *ctx, const double *corners, const int *nlay, const double *ztop,
+                       const double *lsig, int maxl);
+int emg_assemble_rhs_mt(emg_context *ctx, int fidx, int mode, double *s_re, double *s_im);
+int emg_assemble_rhs_csem(emg_context *ctx, int fidx, const double *tx7, const int *dipole_tets,
+                          double *s_re, double *s_im);
+int emg_assemble_rhs_dual(emg_context *ctx, int n_rx, const double *rx, const int *rx_tets, double *s_re,
+                          double *s_im);
+
+/* estimate_error (src/em_fwd.cc:1102-1180) on the named slots: MT (tidx<0)
+ * uses XY, YX and DUAL and writes err[0..T) = sqrt(eta_xy*eta_dual),
+ * err[T..2T) = sqrt(eta_yx*eta_dual); CSEM writes err[0..T).  eta_raw
+ * (optional, n_sol x T) receives the per-solution indicators. */
+int emg_estimate_error(emg_context *ctx, int fidx, int tidx, double *err, double *eta_raw);
+
+/* refine_fixed_fraction / refine_fixed_number (src/em_fwd.cc:1182-1240):
+ * ORs flags into flag[n] exactly as the reference. Host-side. */
+int emg_refine_fixed_fraction(int n, const double *err, double fraction, unsigned char *flag);
+int emg_refine_fixed_number(int n, const double *err, double fraction, unsigned char *flag);
+
+/* interpolate_fields (src/em_fwd.cc:719-744) for n points with known
+ * cells: E and H (6 complex, interleaved re/im) per point from slot target. */
+int emg_interpolate_fields(emg_context *ctx, int target, int fidx, int n, const double *pts,
+                           const int *tets, double *eh);
+
+/* ---- batched fast path (no reference counterpart: replaces the per-task
+ * loop of forward_mt/forward_csem, src/em_fwd.cc:1320-1439) -------------
+ * Solves k right-hand sides with individual frequencies as one block:
+ * complex FGMRES (FP64 outer, true residual in FP64) around an AMS-
+ * preconditioned FCG whose precision is set by -emg_inner_precision
+ * (fp32|fp64).  One AMS hierarchy serves every frequency.
+ * rhs/x: n x k complex, row-major with interleaved re/im (x[(i*k+c)*2+0/1]).
+ * The system solved per column c is the reference's: (C + i w_c Ms) z = conj(s).
+ * x holds the initial guess on entry when use_guess != 0. */
+typedef struct emg_block_opts {
+  double rtol;           /* outer relative residual target (1e-8)           */
+  int max_it;            /* outer iteration cap per column                   */
+  int use_guess;         /* 1: x is the initial guess                        */
+  int inner_fp32;        /* 1: FP32 inner solve, 0: FP64                     */
+  int restart;           /* FGMRES restart (30)                              */
+} emg_block_opts;
+
+int emg_solve_block(emg_context *ctx, int k, const double *freqs, const double *rhs, double *x,
+                    const emg_block_opts *opts, emg_solve_info *infos);
+int emg_solve_block_dev(emg_context *ctx, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                        const emg_block_opts *opts, emg_solve_info *infos);
+
+/* ---- kernel-level entry points on device pointers (tests, benchmarks) -- */
+/* y = (C + i w Ms) x  (conj_out=0)  or its conjugate (conj_out=1, the
+ * real-form operator of matshell_mult_a) for k complex columns. */
+int emg_spmv_complex_dev(emg_context *ctx, int k, const double *omegas_host, const double *x_dev,
+                         double *y_dev, int conj_out);
+/* per-kernel device timing of the last call of each kind (ms) */
+int emg_last_kernel_ms(emg_context *ctx, const char *name, double *ms);
+int emg_stream_synchronize(emg_context *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

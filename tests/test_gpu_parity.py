@@ -1,0 +1,232 @@
+"""GPU parity of every hot-path function against the CPU oracle (C-ABI calls).
+
+Tolerances (written per test):
+  * integer/index work -- sparsity pattern, boundary-cell flags, refine flags:
+    bit-exact;
+  * assembly, operator apply, RHS, estimator: FP64 with a different summation
+    order (atomics, closed-form instead of quadrature) -> 1e-12 relative to the
+    largest entry of the array;
+  * solves: true relative residual <= rtol in FP64, receiver fields within
+    1e-6 relative of the oracle's FP64 solve.
+"""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as sla
+
+import emfem_b200 as E
+from emfem_b200 import meshgen as mg
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(prob, tidx=-3):
+    c = E.EMContext(0)
+    c.set_mesh(prob.mesh)
+    c.set_model(prob.model)
+    c.set_frequencies(prob.survey.freqs)
+    c.create_linear_system(tidx)
+    return c
+
+
+def _close(a, b, tol):
+    scale = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / scale <= tol
+
+
+@pytest.mark.parametrize("name", ["mt_small", "mt_aniso", "csem_small"])
+def test_sparsity_and_assembly(name, request):
+    prob = request.getfixturevalue(name)
+    om = O.Mesh(prob.mesh)
+    orp, oci = O.sparsity(om)
+    with _ctx(prob) as c:
+        rp, ci = c.make_sparsity_patterns()
+        assert np.array_equal(rp, orp)
+        assert np.array_equal(ci, oci)
+        for fidx, f in enumerate(prob.survey.freqs):
+            c.assemble_matrix(fidx)
+            Cg, Mg, bdr = c.get_matrices()
+            Co, Mo, bo = O.assemble(om, prob.model, f, orp, oci)
+            assert np.array_equal(bdr, bo)
+            assert _close(Cg, Co, 1e-12)
+            assert _close(Mg, Mo, 1e-12)
+
+
+def test_matshell_mult_a(mt_small):
+    prob = mt_small
+    om = O.Mesh(prob.mesh)
+    orp, oci = O.sparsity(om)
+    rng = np.random.default_rng(1)
+    with _ctx(prob) as c:
+        c.assemble_matrix(1)
+        Co, Mo, _ = O.assemble(om, prob.model, prob.survey.freqs[1], orp, oci)
+        x = rng.standard_normal(2 * om.ne)
+        y = c.matshell_mult_a(x)
+        yo = O.matshell_mult(orp, oci, Co, Mo, x)
+        assert _close(y, yo, 1e-12)
+
+
+def test_rhs_mt_dual_csem(mt_small, csem_small):
+    prob = mt_small
+    om = O.Mesh(prob.mesh)
+    orp, oci = O.sparsity(om)
+    bg = mg.background_model(prob.mesh, prob.model)
+    with _ctx(prob) as c:
+        c.set_background(*bg)
+        for fidx, f in enumerate(prob.survey.freqs):
+            c.assemble_matrix(fidx)
+            _, _, bo = O.assemble(om, prob.model, f, orp, oci)
+            obg = O.background_model(om, prob.model)
+            for mode in (E.XY_POLAR, E.YX_POLAR):
+                sr, si = c.assemble_rhs_mt(fidx, mode)
+                osr, osi = O.rhs_mt(om, prob.model, f, mode, obg, bo)
+                z, zo = sr + 1j * si, osr + 1j * osi
+                assert _close(z, zo, 1e-12)
+        rx = prob.survey.rx
+        tets = mg.PointLocator(prob.mesh).locate_all(rx)
+        assert (tets >= 0).all()
+        sr, si = c.assemble_rhs_dual(rx, tets)
+        osr, osi = O.rhs_dual(om, rx)
+        assert _close(sr, osr, 1e-12) and _close(si, osi, 1e-12)
+    prob = csem_small
+    om = O.Mesh(prob.mesh)
+    with _ctx(prob, tidx=0) as c:
+        tx = prob.survey.tx[0]
+        tets = mg.PointLocator(prob.mesh).locate_all(tx[None, :3])
+        sr, si = c.assemble_rhs_csem(0, tx, tets)
+        osr, osi = O.rhs_csem(om, prob.survey.freqs[0], tx)
+        assert np.abs(sr).max() == 0.0
+        assert _close(si, osi, 1e-12)
+
+
+def _direct(rp, ci, Cv, Mv, sr, si):
+    A = sp.csr_matrix((Cv + 1j * Mv, ci, rp)).tocsc()
+    return sla.spsolve(A, sr - 1j * si)
+
+
+def test_plain_solve_matches_direct_solution(mt_small):
+    prob = mt_small
+    om = O.Mesh(prob.mesh)
+    orp, oci = O.sparsity(om)
+    bg = mg.background_model(prob.mesh, prob.model)
+    with _ctx(prob) as c:
+        c.set_background(*bg)
+        c.assemble_matrix(1)
+        Co, Mo, _ = O.assemble(om, prob.model, prob.survey.freqs[1], orp, oci)
+        c.create_pc()
+        for mode in (E.XY_POLAR, E.YX_POLAR):
+            sr, si = c.assemble_rhs_mt(1, mode)
+            info = c.solve_linear_system(mode, sr, si, 100, 1e-8)
+            assert info.reason == 0 and info.true_rel_res <= 1e-8
+            er, ei = c.get_solution(mode)
+            z = _direct(orp, oci, Co, Mo, sr, si)
+            assert np.abs((er + 1j * ei) - z).max() / np.abs(z).max() < 1e-6
+            # receiver fields (E, H) within 1e-6 of the exact discrete solution
+            rx = prob.survey.rx[::37]
+            tets = mg.PointLocator(prob.mesh).locate_all(rx)
+            Eg, Hg = c.interpolate_fields(mode, 1, rx, tets)
+            for i in range(len(rx)):
+                Eo, Ho = O.interpolate_fields(om, int(tets[i]), rx[i], prob.survey.freqs[1], z.real, z.imag)
+                assert np.abs(Eg[i] - Eo).max() <= 1e-6 * np.abs(Eo).max()
+                assert np.abs(Hg[i] - Ho).max() <= 1e-6 * np.abs(Ho).max()
+
+
+def test_pc_apply_reaches_inner_tolerance(mt_small):
+    prob = mt_small
+    om = O.Mesh(prob.mesh)
+    orp, oci = O.sparsity(om)
+    rng = np.random.default_rng(3)
+    with _ctx(prob) as c:
+        c.assemble_matrix(2)
+        Co, Mo, _ = O.assemble(om, prob.model, prob.survey.freqs[2], orp, oci)
+        c.create_pc()
+        B = sp.csr_matrix((Co + Mo, oci, orp))
+        b = rng.standard_normal(2 * om.ne)
+        x = c.pc_apply_b(b)
+        n = om.ne
+        for h in (slice(0, n), slice(n, 2 * n)):
+            r = b[h] - B @ x[h]
+            assert np.linalg.norm(r) <= 1e-2 * np.linalg.norm(b[h]) * (1 + 1e-9)
+
+
+def test_solver_reports_divergence(mt_small):
+    prob = mt_small
+    bg = mg.background_model(prob.mesh, prob.model)
+    with _ctx(prob) as c:
+        c.set_background(*bg)
+        c.assemble_matrix(0)
+        c.create_pc()
+        sr, si = c.assemble_rhs_mt(0, E.XY_POLAR)
+        with pytest.raises(E.EMGError) as ei:
+            c.solve_linear_system(E.XY_POLAR, sr, si, 1, 1e-12)
+        assert ei.value.code == E.api.EMG_DIVERGED_ITS
+        info = c.solve_linear_system(E.XY_POLAR, np.zeros_like(sr), np.zeros_like(si), 10, 1e-8)
+        er, ei_ = c.get_solution(E.XY_POLAR)
+        assert info.reason == 0 and np.abs(er).max() == 0 and np.abs(ei_).max() == 0
+
+
+def test_estimator_and_refine_flags(mt_small):
+    prob = mt_small
+    om = O.Mesh(prob.mesh)
+    orp, oci = O.sparsity(om)
+    bg = mg.background_model(prob.mesh, prob.model)
+    f = prob.survey.freqs[1]
+    rx = prob.survey.rx
+    tets = mg.PointLocator(prob.mesh).locate_all(rx)
+    with _ctx(prob) as c:
+        c.set_background(*bg)
+        c.assemble_matrix(1)
+        Co, Mo, bo = O.assemble(om, prob.model, f, orp, oci)
+        obg = O.background_model(om, prob.model)
+        sols = []
+        for mode in (E.XY_POLAR, E.YX_POLAR):
+            sr, si = O.rhs_mt(om, prob.model, f, mode, obg, bo)
+            z = _direct(orp, oci, Co, Mo, sr, si)
+            c.set_solution(mode, z.real, z.imag)
+            sols.append((z.real, z.imag))
+        sr, si = O.rhs_dual(om, rx)
+        z = _direct(orp, oci, Co, Mo, sr, si)
+        c.set_solution(E.SOL_DUAL, z.real, z.imag)
+        sols.append((z.real, z.imag))
+        err, eta = c.estimate_error(1, -3)
+        eta_o = O.estimate(om, prob.model, f, sols)
+        for s in range(3):
+            assert _close(eta[s], eta_o[s], 1e-10)
+        err_o = np.sqrt(eta_o[:2] * eta_o[2])
+        assert _close(err, err_o, 1e-10)
+        for frac in (0.1, 0.3):
+            fg = E.refine_fixed_fraction(err[0], frac)
+            E.refine_fixed_fraction(err[1], frac, fg)
+            fo = O.refine_fixed_fraction(err_o[0], frac)
+            O.refine_fixed_fraction(err_o[1], frac, fo)
+            assert np.array_equal(fg, fo)
+            fg = E.refine_fixed_number(err[0], frac)
+            fo = O.refine_fixed_number(err_o[0], frac)
+            assert np.array_equal(fg, fo)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_block_solve_matches_plain(mt_small, fp32):
+    prob = mt_small
+    bg = mg.background_model(prob.mesh, prob.model)
+    om = O.Mesh(prob.mesh)
+    orp, oci = O.sparsity(om)
+    with _ctx(prob) as c:
+        c.set_background(*bg)
+        cols, freqs, ref = [], [], []
+        for fidx in (0, 2):
+            c.assemble_matrix(fidx)
+            f = prob.survey.freqs[fidx]
+            Co, Mo, _ = O.assemble(om, prob.model, f, orp, oci)
+            for mode in (E.XY_POLAR, E.YX_POLAR):
+                sr, si = c.assemble_rhs_mt(fidx, mode)
+                cols.append(sr + 1j * si)
+                freqs.append(f)
+                ref.append(_direct(orp, oci, Co, Mo, sr, si))
+        rhs = np.stack(cols, axis=1)
+        x, infos = c.solve_block(freqs, rhs, rtol=1e-8, max_it=200, inner_fp32=fp32)
+        for j in range(len(freqs)):
+            assert infos[j].reason == 0 and infos[j].true_rel_res <= 1e-8
+            assert np.abs(x[:, j] - ref[j]).max() / np.abs(ref[j]).max() < 1e-6
