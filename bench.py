@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark: right-hand sides solved per second to 1e-8 relative residual.
+
+Workload (default): the batched + mixed-precision MT configuration with
+topography -- ~1.5M tets, 8 frequencies log-spaced in [1e-3, 100] Hz x 2
+polarisations = 16 right-hand sides solved as one block (synthetic seeded
+mesh/model from emfem_b200.meshgen).  One step = the hot path
+over that batch: assemble_matrix, AMS setup, MT right-hand sides, block
+FGMRES(FCG(AMS)) solve with FP64 outer iterations and an FP32 AMS.
+
+value  : RHS/s with inputs resident on the device (device-timed, CUDA events)
+e2e    : RHS/s through the host-buffer C ABI (emg_assemble_rhs_mt_block +
+         emg_solve_block), host<->device copies inside the timed region
+plain_fp64 : the per-RHS FP64 drop-in (real-form FGMRES, per-frequency AMS
+         setup, zero guess) on a subset of the same columns, for the ratio
+roofline : the edge-operator SpMM inside the AMS (dominant kernel), achieved
+         algorithmic GB/s from live CUDA-event profiling over the timed region
+cpu_baseline : the CPU oracle (restatement of the reference path) on a bounded
+         sample of the same workload, rank 0, N=1 only
+
+--impl reference times the CPU oracle alone (the reference's own MPI/PETSc
+binary cannot be built in this image) and prints the same line with
+"impl": "reference".
+"""
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RHS solved/s at 1e-8 residual: mixed+batched+warm-start vs plain FP64 (1 B200)"
+UNIT = "RHS/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--plain-freqs", type=int, default=2, help="frequencies timed on the plain FP64 path")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--breakdown", action="store_true", help="print per-phase host timings to stderr")
+    return ap.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def columns(prob):
+    freqs = np.asarray(prob.survey.freqs, dtype=np.float64)
+    colf = np.repeat(freqs, 2)
+    modes = np.tile(np.array([-1, -2], dtype=np.int32), freqs.size)
+    return freqs, colf, modes
+
+
+def roofline_traffic(bin_name):
+    """DRAM traffic per launch of the profiled kernel from the committed ncu
+    summary (profiles/<bin>_traffic.txt, line 'traffic_bytes_per_launch: X')."""
+    path = os.path.join(ROOT, "profiles", bin_name + "_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------------------
+# CPU oracle baseline (bounded sample)
+# ----------------------------------------------------------------------------
+def cpu_sample(prob, n_rhs_per_setup=2, max_outer=1):
+    """Times the oracle on one frequency of the workload: assembly, AMS setup
+    and `max_outer` FGMRES iterations of one RHS.  Returns the measured times."""
+    import oracle as O
+    threads = O.num_threads(0)
+    m = O.Mesh(prob.mesh)
+    rp, ci = O.sparsity(m)
+    f = float(prob.survey.freqs[0])
+    t0 = time.perf_counter()
+    Cv, Mv, bdr = O.assemble(m, prob.model, f, rp, ci)
+    t_asm = time.perf_counter() - t0
+    obg = O.background_model(m, prob.model)
+    t0 = time.perf_counter()
+    sr, si = O.rhs_mt(m, prob.model, f, -1, obg, bdr)
+    t_rhs = time.perf_counter() - t0
+    er, ei, its, st = O.solve(m, rp, ci, Cv, Mv, sr, si, 1e-8, max_outer)
+    return dict(threads=threads, t_asm=t_asm, t_rhs=t_rhs, t_setup=float(st[2]), t_fgmres=float(st[3]),
+                outer=int(its), inner=int(st[1]))
+
+
+def cpu_calibration(cfg):
+    """Iteration counts of full oracle solves on this workload (committed)."""
+    path = os.path.join(ROOT, "oracle", "calibration_cfg%d.json" % cfg)
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_rhs_per_s(sample, inner_per_rhs):
+    t_inner = sample["t_fgmres"] / max(sample["inner"], 1)
+    per_rhs = (sample["t_asm"] + sample["t_setup"]) / 2.0 + sample["t_rhs"] + inner_per_rhs * t_inner
+    return 1.0 / per_rhs, per_rhs
+
+
+def reference_arm(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        barrier(world)
+        return
+    from emfem_b200 import meshgen as mg
+    prob = mg.config(args.config, args.scale)
+    cal = cpu_calibration(args.config)
+    inner = cal["inner_per_rhs"] if cal else None
+    samples = []
+    for _ in range(args.warmup):
+        cpu_sample(prob)
+    for _ in range(args.steps):
+        samples.append(cpu_sample(prob))
+    if inner is None:
+        inner = 30 * samples[0]["inner"]
+    vals = [cpu_rhs_per_s(s, inner)[0] for s in samples]
+    v = float(np.median(vals))
+    per_rhs = 1.0 / v
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_rhs * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": prob.name, "tets": prob.mesh.n_tets, "edges": prob.mesh.n_edges,
+                   "rhs": 2 * len(prob.survey.freqs), "rtol": 1e-8},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": samples[0]["threads"], "kind": "port",
+                         "sample": ("CPU oracle (C++ restatement of the reference path; the PETSc/hypre "
+                                    "binary cannot be built here): per step one frequency of the workload -- "
+                                    "assembly, AMS setup, MT RHS and one FGMRES iteration of one RHS; RHS/s = "
+                                    "1/((asm+setup)/2 + rhs + inner_its_per_rhs x time per inner iteration), "
+                                    "inner_its_per_rhs=%s from %s" % (inner, "committed full oracle solves"
+                                                                       if cal else "30 x sampled"))},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+def ours(args):
+    world, rank, local = dist_setup()
+    import torch
+    import emfem_b200 as E
+    from emfem_b200 import meshgen as mg
+
+    torch.cuda.set_device(local)
+    prob = mg.config(args.config, args.scale)
+    freqs, colf, modes = columns(prob)
+    K = colf.size
+    bg = mg.background_model(prob.mesh, prob.model)
+    ctx = E.EMContext(local)
+    ctx.set_mesh(prob.mesh)
+    ctx.set_model(prob.model)
+    ctx.set_frequencies(freqs)
+    ctx.create_linear_system(-3)
+    ctx.set_background(*bg)
+    ne = prob.mesh.n_edges
+    rhs = torch.zeros((ne, K), dtype=torch.complex128, device="cuda")
+    x = torch.zeros((ne, K), dtype=torch.complex128, device="cuda")
+    torch.cuda.synchronize()
+    infos_last = []
+    breakdown = {}
+
+    def step():
+        nonlocal infos_last
+        t0 = time.perf_counter()
+        ctx.assemble_matrix(0)
+        t1 = time.perf_counter()
+        ctx.assemble_rhs_mt_block_dev(colf, modes, rhs.data_ptr())
+        t2 = time.perf_counter()
+        infos_last = ctx.solve_block_dev(colf, rhs.data_ptr(), x.data_ptr(), rtol=1e-8, max_it=200,
+                                         inner_fp32=True)
+        t3 = time.perf_counter()
+        for k, v in (("assemble", t1 - t0), ("rhs", t2 - t1), ("setup+solve", t3 - t2)):
+            breakdown[k] = breakdown.get(k, 0.0) + v
+
+    for _ in range(args.warmup):
+        step()
+    breakdown.clear()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    E.profile_enable(True)
+    l0 = E.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    launches = E.launch_count() - l0
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms, world)
+    barrier(world)
+    ms_step = ms / args.steps
+    value = world * K * args.steps / (ms / 1e3)
+    bins = {}
+    for b in ("spmm_edge_fp32", "spmm_edge_fp64", "spmm_nodal_fp32"):
+        n, t, by = E.profile_get(b)
+        bins[b] = (n, t, by)
+    E.profile_enable(False)
+    conv = [(i.true_rel_res, i.outer_its) for i in infos_last]
+    all_conv = all(i.reason == 0 and i.true_rel_res <= 1e-8 for i in infos_last)
+    dom = max(bins, key=lambda b: bins[b][1])
+    n_l, t_l, b_l = bins[dom]
+    peak, peak_kind = peaks()
+    achieved = (b_l / max(n_l, 1)) / ((t_l / max(n_l, 1)) * 1e-3) / 1e9 if n_l else 0.0
+    traffic = roofline_traffic(dom)
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+            "algorithmic_bytes_per_launch": b_l / max(n_l, 1), "launches": n_l,
+            "avg_launch_us": 1e3 * t_l / max(n_l, 1),
+            "share_of_step": t_l / ms if ms > 0 else None}
+
+    # ---- e2e through the host-buffer C ABI ----------------------------------
+    e2e = None
+    if not args.no_e2e:
+        h_x = np.zeros((ne, K), dtype=np.complex128)
+        torch.cuda.synchronize()
+        barrier(world)
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.assemble_matrix(0)
+            h_rhs = ctx.assemble_rhs_mt_block(colf, modes)
+            h_x, _ = ctx.solve_block(colf, h_rhs, rtol=1e-8, max_it=200, inner_fp32=True)
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(time.perf_counter() - w0, world)
+        nbytes = ne * K * 16
+        e2e = {"value": world * K * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": 2 * nbytes,
+               "path": "emg_assemble_rhs_mt_block (D2H) + emg_solve_block (H2D rhs, D2H x), host wall clock"}
+
+    # ---- plain FP64 drop-in on a subset of the columns ----------------------
+    plain = None
+    if args.plain_freqs > 0:
+        idx = np.unique(np.linspace(0, freqs.size - 1, args.plain_freqs).round().astype(int))
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        p_info = []
+        for fi in idx:
+            ctx.assemble_matrix(int(fi))
+            ctx.create_pc()
+            for mode in (E.XY_POLAR, E.YX_POLAR):
+                sr, si = ctx.assemble_rhs_mt(int(fi), mode)
+                inf = ctx.solve_linear_system(mode, sr, si, 300, 1e-8, raise_on_diverge=False)
+                p_info.append(inf.as_dict())
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - w0
+        n_plain = 2 * len(idx)
+        plain = {"value": n_plain / t_plain, "unit": UNIT, "rhs": n_plain, "freqs": [float(freqs[i]) for i in idx],
+                 "outer_its": [p["outer_its"] for p in p_info], "inner_its": [p["inner_its"] for p in p_info],
+                 "true_rel_res": [p["true_rel_res"] for p in p_info],
+                 "timing": "host wall clock around assemble_matrix + create_pc + 2 x (rhs + solve) per frequency"}
+
+    # ---- CPU baseline --------------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            s = cpu_sample(prob)
+            cal = cpu_calibration(args.config)
+            if cal:
+                inner, src = cal["inner_per_rhs"], "committed full oracle solves of this workload"
+            elif plain:
+                inner, src = float(np.mean(plain["inner_its"])) / 2.0, "GPU plain path inner counts"
+            else:
+                inner, src = 30 * s["inner"], "30 x sampled"
+            v, per_rhs = cpu_rhs_per_s(s, inner)
+            cpu = {"value": v, "unit": UNIT, "cores": s["threads"], "kind": "port",
+                   "sample": ("CPU oracle on one frequency of this workload: assembly %.2fs, AMS setup %.2fs, "
+                              "MT RHS %.2fs, %d FGMRES iteration(s) with %d inner FCG iterations in %.2fs; "
+                              "RHS/s = 1/((asm+setup)/2 + rhs + %.1f inner its per RHS (%s) x time per inner "
+                              "iteration)" % (s["t_asm"], s["t_setup"], s["t_rhs"], s["outer"], s["inner"],
+                                              s["t_fgmres"], inner, src))}
+        except Exception as ex:  # the baseline must not kill the benchmark line
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": "failed: %s" % ex}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 outer / f32 AMS", "data": "synthetic",
+            "config": {"workload": prob.name, "tets": prob.mesh.n_tets, "edges": prob.mesh.n_edges,
+                       "nnz": int(ctx.make_sparsity_patterns()[0][-1]), "rhs_per_step": K, "freqs_hz":
+                       [float(f) for f in freqs], "rtol": 1e-8, "inner": "FCG(FP64) + AMS(FP32)",
+                       "warm_start": "none (zero guess)", "l2": "inputs larger than L2 (operator ~%.0f MB)" %
+                       (int(ctx.make_sparsity_patterns()[0][-1]) * 20 / 1e6), "parallelism": "replicas" if world > 1 else "1 GPU"},
+            "e2e": e2e, "plain_fp64": plain,
+            "speedup_vs_plain_fp64": (value / world) / plain["value"] if plain else None,
+            "converged": all_conv, "true_rel_res_max": max(c[0] for c in conv) if conv else None,
+            "outer_its": [c[1] for c in conv],
+            "roofline": roof, "profile_bins": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in bins.items()},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "wall_s": wall,
+        }
+        print(json.dumps(line), flush=True)
+        if args.breakdown:
+            print("breakdown (s over %d steps): %s" % (args.steps, breakdown), file=sys.stderr)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

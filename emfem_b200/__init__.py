@@ -8,8 +8,9 @@ library or without a GPU every compute call raises.
 """
 
 from .api import (EMContext, EMGError, SolveInfo, lib, library_path, refine_fixed_fraction,
-                  refine_fixed_number, XY_POLAR, YX_POLAR, SOL_CSEM, SOL_DUAL)
+                  refine_fixed_number, launch_count, profile_enable, profile_get, XY_POLAR, YX_POLAR,
+                  SOL_CSEM, SOL_DUAL)
 from . import meshgen
 
 __all__ = ["EMContext", "EMGError", "SolveInfo", "lib", "library_path", "refine_fixed_fraction",
-           "refine_fixed_number", "XY_POLAR", "YX_POLAR", "SOL_CSEM", "SOL_DUAL", "meshgen"]
+           "refine_fixed_number", "launch_count", "profile_enable", "profile_get", "XY_POLAR", "YX_POLAR", "SOL_CSEM", "SOL_DUAL", "meshgen"]

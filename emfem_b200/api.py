@@ -91,6 +91,11 @@ _SIGS = {
     "emg_spmv_complex_dev": ([_P, _I, _P, _P, _P, _I], _I),
     "emg_last_kernel_ms": ([_P, C.c_char_p, C.POINTER(_D)], _I),
     "emg_stream_synchronize": ([_P], _I),
+    "emg_launch_count": ([C.POINTER(C.c_long)], _I),
+    "emg_profile_enable": ([_I], _I),
+    "emg_profile_get": ([C.c_char_p, C.POINTER(C.c_long), C.POINTER(_D), C.POINTER(_D)], _I),
+    "emg_assemble_rhs_mt_block": ([_P, _I, _P, _P, _P], _I),
+    "emg_assemble_rhs_mt_block_dev": ([_P, _I, _P, _P, _P], _I),
 }
 
 
@@ -126,6 +131,23 @@ def _f64(a):
 
 def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def launch_count() -> int:
+    n = C.c_long()
+    _check(lib().emg_launch_count(C.byref(n)))
+    return n.value
+
+
+def profile_enable(on=True):
+    _check(lib().emg_profile_enable(int(on)))
+
+
+def profile_get(bin_name):
+    """(launches, device ms, algorithmic bytes) accumulated in a profiler bin."""
+    n, ms, by = C.c_long(), C.c_double(), C.c_double()
+    _check(lib().emg_profile_get(bin_name.encode(), C.byref(n), C.byref(ms), C.byref(by)))
+    return n.value, ms.value, by.value
 
 
 def refine_fixed_fraction(err, fraction, flag=None):
@@ -308,6 +330,21 @@ class EMContext:
         o = out.reshape(-1, 6, 2)
         z = o[..., 0] + 1j * o[..., 1]
         return z[:, :3], z[:, 3:]
+
+    def assemble_rhs_mt_block(self, freqs, modes):
+        """k MT right-hand sides at once: returns (n, k) complex."""
+        freqs = _f64(freqs)
+        modes = _i32(modes)
+        out = np.zeros((self.ne, freqs.size), dtype=np.complex128)
+        _check(lib().emg_assemble_rhs_mt_block(self._h, freqs.size, _ptr(freqs), _ptr(modes),
+                                               _ptr(out.view(np.float64))))
+        return out
+
+    def assemble_rhs_mt_block_dev(self, freqs, modes, s_ptr):
+        freqs = _f64(freqs)
+        modes = _i32(modes)
+        _check(lib().emg_assemble_rhs_mt_block_dev(self._h, freqs.size, _ptr(freqs), _ptr(modes),
+                                                   C.c_void_p(s_ptr)))
 
     # -- batched fast path ----------------------------------------------------------------
     @staticmethod

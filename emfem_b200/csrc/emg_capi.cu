@@ -12,6 +12,7 @@
 #include <sstream>
 #include <string>
 #include <array>
+#include <atomic>
 
 #include "emg_internal.h"
 #include "emg_kernels.cuh"
@@ -29,6 +30,57 @@ void fail(int code, const char *fmt, ...) {
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
   throw Error(code, buf);
+}
+
+static std::atomic<long> g_launches{0};
+long launch_count() { return g_launches.load(); }
+
+void launch_check(const char *file, int line) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  check_cuda(cudaGetLastError(), "kernel launch", file, line);
+}
+
+KernelProfiler &profiler() {
+  static KernelProfiler p;
+  return p;
+}
+
+void KernelProfiler::begin(const std::string &bin, cudaStream_t s, double algo_bytes, cudaEvent_t *start_out) {
+  cudaEvent_t a, b;
+  EMG_CUDA(cudaEventCreate(&a));
+  EMG_CUDA(cudaEventCreate(&b));
+  EMG_CUDA(cudaEventRecord(a, s));
+  open[bin].push_back(Rec{a, b, algo_bytes});
+  *start_out = a;
+}
+
+void KernelProfiler::end(const std::string &bin, cudaStream_t s, cudaEvent_t start) {
+  auto &v = open[bin];
+  if (v.empty() || v.back().a != start) fail(EMG_ERR_STATE, "profiler: unbalanced records");
+  EMG_CUDA(cudaEventRecord(v.back().b, s));
+}
+
+void KernelProfiler::collect() {
+  for (auto &kv : open) {
+    for (auto &r : kv.second) {
+      EMG_CUDA(cudaEventSynchronize(r.b));
+      float t = 0;
+      EMG_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+      ms[kv.first] += t;
+      bytes[kv.first] += r.bytes;
+      count[kv.first] += 1;
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    kv.second.clear();
+  }
+}
+
+void KernelProfiler::reset() {
+  collect();
+  ms.clear();
+  bytes.clear();
+  count.clear();
 }
 
 void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
@@ -153,6 +205,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_amg_max_levels") o.amg_max_levels = geti(k, v);
     else if (key == "emg_amg_relax_times") o.amg_relax_times = geti(k, v);
     else if (key == "emg_amg_pmax") o.amg_pmax = geti(k, v);
+    else if (key == "emg_smoother") o.smoother_cheb = elist(k, v, {"l1jacobi", "chebyshev"});
     else if (key == "emg_graphs") o.graphs = v.empty() ? 1 : getb(v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
     else if (key.rfind("A_", 0) == 0 || key.rfind("B_", 0) == 0) ignored.push_back(k);
@@ -1074,7 +1127,12 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     a.y = s_;
     a.relax_w = 1.0;
     a.mode = SPMM_AX;
+    KernelProfiler &pf = profiler();
+    cudaEvent_t ev = nullptr;
+    if (pf.enabled)
+      pf.begin("spmm_edge_fp64", c.stream, spmm_algo_bytes(n, c.nnz, K2, 8, true, SPMM_AX), &ev);
     spmm_nnz<double>(K2, a, c.nnz, c.stream);
+    if (pf.enabled) pf.end("spmm_edge_fp64", c.stream, ev);
   };
   auto pc32 = [&](const double *r_, double *z_) {
     cvt_d2f((long)n * K2, r_, w.f_in.p, c.stream);
@@ -1142,6 +1200,57 @@ int emg_last_kernel_ms(emg_context *c, const char *name, double *ms) {
 int emg_stream_synchronize(emg_context *c) {
   EMG_API_BEGIN
   need(c != nullptr, EMG_ERR_ARG, "null context");
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  EMG_API_END
+}
+
+int emg_launch_count(long *n) {
+  EMG_API_BEGIN
+  need(n != nullptr, EMG_ERR_ARG, "null argument");
+  *n = launch_count();
+  EMG_API_END
+}
+
+int emg_profile_enable(int on) {
+  EMG_API_BEGIN
+  KernelProfiler &p = profiler();
+  p.reset();
+  p.enabled = on != 0;
+  EMG_API_END
+}
+
+int emg_profile_get(const char *bin, long *count, double *ms, double *bytes) {
+  EMG_API_BEGIN
+  need(bin && count && ms && bytes, EMG_ERR_ARG, "null argument");
+  KernelProfiler &p = profiler();
+  p.collect();
+  *count = p.count.count(bin) ? p.count[bin] : 0;
+  *ms = p.ms.count(bin) ? p.ms[bin] : 0.0;
+  *bytes = p.bytes.count(bin) ? p.bytes[bin] : 0.0;
+  EMG_API_END
+}
+
+// batched MT right-hand sides on the device: column j is polarisation
+// modes[j] at frequency freqs[j]; out: n x k complex interleaved
+int emg_assemble_rhs_mt_block_dev(emg_context *c, int k, const double *freqs, const int *modes, double *s_dev) {
+  EMG_API_BEGIN
+  need(c && freqs && modes && s_dev && k > 0, EMG_ERR_ARG, "null argument");
+  need(c->assembled, EMG_ERR_STATE, "assemble_rhs_mt before assemble_matrix");
+  for (int j = 0; j < k; ++j)
+    need(modes[j] == EMG_SOL_MT_XY || modes[j] == EMG_SOL_MT_YX, EMG_ERR_ARG, "mode must be XY_POLAR or YX_POLAR");
+  EMG_CUDA(cudaSetDevice(c->device));
+  rhs_mt_block(*c, k, freqs, modes, s_dev);
+  EMG_API_END
+}
+
+int emg_assemble_rhs_mt_block(emg_context *c, int k, const double *freqs, const int *modes, double *s) {
+  EMG_API_BEGIN
+  need(c && freqs && modes && s && k > 0, EMG_ERR_ARG, "null argument");
+  need(c->assembled, EMG_ERR_STATE, "assemble_rhs_mt before assemble_matrix");
+  EMG_CUDA(cudaSetDevice(c->device));
+  DBuf<double> d((size_t)c->ne * k * 2);
+  rhs_mt_block(*c, k, freqs, modes, d.p);
+  d.download(s, (size_t)c->ne * k * 2, c->stream);
   EMG_CUDA(cudaStreamSynchronize(c->stream));
   EMG_API_END
 }

@@ -31,7 +31,29 @@ struct Error : public std::runtime_error {
 [[noreturn]] void fail(int code, const char *fmt, ...);
 void check_cuda(cudaError_t e, const char *what, const char *file, int line);
 #define EMG_CUDA(x) ::emg::check_cuda((x), #x, __FILE__, __LINE__)
-#define EMG_LAUNCH_CHECK() ::emg::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+// every kernel launch is followed by this check, which also counts launches
+void launch_check(const char *file, int line);
+#define EMG_LAUNCH_CHECK() ::emg::launch_check(__FILE__, __LINE__)
+
+// Event-based per-kernel profiler: bins named by kernel role; each record is a
+// start/stop event pair on the launching stream plus the launch's
+// algorithmic bytes.  Disabled unless enabled through the C ABI.
+struct KernelProfiler {
+  bool enabled = false;
+  struct Rec {
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  std::map<std::string, std::vector<Rec>> open;
+  std::map<std::string, double> ms, bytes;
+  std::map<std::string, long> count;
+  void begin(const std::string &bin, cudaStream_t s, double algo_bytes, cudaEvent_t *start_out);
+  void end(const std::string &bin, cudaStream_t s, cudaEvent_t start);
+  void collect();  // synchronizes on the recorded events and folds them in
+  void reset();
+};
+KernelProfiler &profiler();
+long launch_count();
 
 // ---------------------------------------------------------------------------
 // device buffer (cudaMalloc-backed, move-only)
@@ -128,6 +150,7 @@ struct Options {
   int amg_max_coarse = 200;
   int amg_max_levels = 25;
   int amg_relax_times = 1;
+  int smoother_cheb = 1;  // degree-2 Chebyshev (1) or l1-Jacobi (0) in AMS and AMG
   // emg_*
   int inner_fp32 = 0;
   int graphs = 1;

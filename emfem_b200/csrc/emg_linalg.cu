@@ -116,7 +116,8 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
     cfg = spmm_default<T>(K, a.n ? (double)nnz / a.n : 1.0);
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     EMG_CUDA(cudaStreamIsCapturing(s, &cs));
-    if (tn.allow_tuning && cs == cudaStreamCaptureStatusNone && a.mode != SPMM_ADD && a.n >= 20000) {
+    const bool idempotent = a.mode == SPMM_AX || a.mode == SPMM_RES || a.mode == SPMM_JAC || a.mode == SPMM_CHEB1;
+    if (tn.allow_tuning && cs == cudaStreamCaptureStatusNone && idempotent && a.n >= 20000) {
       cudaEvent_t e0, e1;
       EMG_CUDA(cudaEventCreate(&e0));
       EMG_CUDA(cudaEventCreate(&e1));
@@ -148,6 +149,18 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
 
 template void spmm_nnz<float>(int, const SpmmArgs &, long, cudaStream_t);
 template void spmm_nnz<double>(int, const SpmmArgs &, long, cudaStream_t);
+
+double spmm_algo_bytes(long n, long nnz, int K, int elem, bool two_parts, int mode) {
+  double b = (double)nnz * (4.0 + elem * (two_parts ? 2 : 1)) + (double)(n + 1) * 4.0;
+  double vec = (double)n * K * elem;
+  b += 2.0 * vec;  // x gathered once, y written once
+  if (mode == SPMM_RES) b += vec;
+  if (mode == SPMM_JAC) b += vec + (double)n * elem * (two_parts ? 2 : 1);
+  if (mode == SPMM_ADD) b += vec;
+  if (mode == SPMM_CHEB1) b += 3.0 * vec + (double)n * elem * (two_parts ? 2 : 1);   // b, x-row in; r, d out
+  if (mode == SPMM_CHEB2) b += 2.0 * vec + (double)n * elem * (two_parts ? 2 : 1);   // r, y-row in
+  return b;
+}
 
 // ---------------------------------------------------------------------------
 // column reductions and vector updates
@@ -289,6 +302,30 @@ void jacobi0(int n, int K, const T *b, const T *l1c, const T *l1m, const double 
   long total = (long)n * K;
   if (!total) return;
   jacobi0_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, b, l1c, l1m, omega, w, y);
+  EMG_LAUNCH_CHECK();
+}
+
+template <typename T>
+__global__ void jacobi0_2_kernel(long total, int K, const T *__restrict__ b, const T *__restrict__ l1c,
+                                 const T *__restrict__ l1m, const double *__restrict__ omega, double w,
+                                 T *__restrict__ y, T *__restrict__ d) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  long row = i / K;
+  int c = (int)(i % K);
+  T dg = l1c[row];
+  if (l1m) dg += (T)omega[c] * l1m[row];
+  T v = (T)w * b[i] / dg;
+  y[i] = v;
+  d[i] = v;
+}
+
+template <typename T>
+void jacobi0_2(int n, int K, const T *b, const T *l1c, const T *l1m, const double *omega, double w, T *y, T *d,
+               cudaStream_t s) {
+  long total = (long)n * K;
+  if (!total) return;
+  jacobi0_2_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, b, l1c, l1m, omega, w, y, d);
   EMG_LAUNCH_CHECK();
 }
 
@@ -615,6 +652,8 @@ void cnorm2(int n, int K, const double *x, double *out, cudaStream_t s) {
   template void fcg_update<T>(int, int, const double *, const T *, const T *, T *, T *, double *, cudaStream_t); \
   template void fcg_direction<T>(int, int, const T *, int, T *const *, const double *, T *, cudaStream_t);       \
   template void jacobi0<T>(int, int, const T *, const T *, const T *, const double *, double, T *, cudaStream_t); \
+  template void jacobi0_2<T>(int, int, const T *, const T *, const T *, const double *, double, T *, T *,           \
+                             cudaStream_t);                                                                      \
   template void fill_zero<T>(long, T *, cudaStream_t);                                                           \
   template void ams_restrict<T>(int, int, int, const int *, const int *, const T *, const T *, T *, cudaStream_t); \
   template void ams_prolong_add<T>(int, int, int, const int *, const T *, const T *, T *, cudaStream_t);          \

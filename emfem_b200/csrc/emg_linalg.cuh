@@ -26,6 +26,10 @@ enum SpmmMode : int {
   SPMM_RES = 1,   // y = b - A x
   SPMM_JAC = 2,   // y = x + w (b - A x) / d,  d = l1c + w_c l1m
   SPMM_ADD = 3,   // y = y + A x   (prolongation)
+  // degree-2 Chebyshev smoothing on D^-1 A (D = l1 row sums, spectrum in
+  // (0, 1]), fused into the two operator applications it needs:
+  SPMM_CHEB1 = 4, // r = b - A x ; d = inv_theta D^-1 r ; y = x + d   (stores r, d)
+  SPMM_CHEB2 = 5, // y += c1 d + c2 D^-1 (r - A d)      (x = d gathered, y in place)
 };
 
 template <typename T, int V>
@@ -74,6 +78,8 @@ struct SpmmArgs {
   void *y;
   double relax_w;
   int mode;
+  void *r, *d;             // Chebyshev work vectors (n x K)
+  double c1, c2;           // Chebyshev coefficients (inv_theta in c1 for CHEB1)
 };
 
 template <typename T, int K, int V, int NL>
@@ -155,11 +161,42 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
     }
     break;
   }
-  default: {  // SPMM_ADD
+  case SPMM_ADD: {
     T yo[V];
     ldv_plain<T, V>(y + o, yo);
 #pragma unroll
     for (int i = 0; i < V; ++i) out[i] = yo[i] + acc[i];
+    break;
+  }
+  case SPMM_CHEB1: {
+    T bv[V], xo[V], rr[V], dd[V];
+    ldv<T, V>(static_cast<const T *>(a.b) + o, bv);
+    ldv<T, V>(x + o, xo);
+    const T dc = __ldg(static_cast<const T *>(a.l1c) + row);
+    const T dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      T dg = two ? dc + w[i] * dm : dc;
+      rr[i] = bv[i] - acc[i];
+      dd[i] = (T)a.c1 * rr[i] / dg;
+      out[i] = xo[i] + dd[i];
+    }
+    stv<T, V>(static_cast<T *>(a.r) + o, rr);
+    stv<T, V>(static_cast<T *>(a.d) + o, dd);
+    break;
+  }
+  default: {  // SPMM_CHEB2: x is d (gathered), r holds the residual
+    T rr[V], dd[V], yo[V];
+    ldv<T, V>(static_cast<const T *>(a.r) + o, rr);
+    ldv<T, V>(x + o, dd);
+    ldv_plain<T, V>(y + o, yo);
+    const T dc = __ldg(static_cast<const T *>(a.l1c) + row);
+    const T dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      T dg = two ? dc + w[i] * dm : dc;
+      out[i] = yo[i] + (T)a.c1 * dd[i] + (T)a.c2 * (rr[i] - acc[i]) / dg;
+    }
   }
   }
   stv<T, V>(y + o, out);

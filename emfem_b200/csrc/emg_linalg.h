@@ -24,6 +24,10 @@ struct SpmmTuner {
 
 SpmmTuner &tuner();
 
+// algorithmic bytes of one SpMM launch: every stored array read or written
+// once (pattern, value parts, x, y, and b / x-row / l1 sums as the mode needs)
+double spmm_algo_bytes(long n, long nnz, int K, int elem, bool two_parts, int mode);
+
 // nnz of the operator selects the row-length class of the tuning table
 template <typename T>
 void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s);
@@ -45,6 +49,10 @@ void fcg_direction(int n, int K, const T *z, int nprev, T *const *Pj, const doub
 template <typename T>
 void jacobi0(int n, int K, const T *b, const T *l1c, const T *l1m, const double *omega, double w, T *y,
              cudaStream_t s);
+// y = d = w * b / D  (first smoothing step from a zero guess, two outputs)
+template <typename T>
+void jacobi0_2(int n, int K, const T *b, const T *l1c, const T *l1m, const double *omega, double w, T *y, T *d,
+               cudaStream_t s);
 // precision conversion of block vectors
 void cvt_d2f(long count, const double *a, float *b, cudaStream_t s);
 void cvt_f2d(long count, const float *a, double *b, cudaStream_t s);

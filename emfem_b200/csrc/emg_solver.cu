@@ -108,7 +108,10 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   ams.relax_times = c.opt.ams_relax_times;
   ams.relax_w = c.opt.ams_relax_weight;
   ams.amg_relax_times = c.opt.amg_relax_times;
+  ams.cheb = c.opt.smoother_cheb;
   ams.two = !per_frequency;
+  ams.use_graphs = c.opt.graphs != 0;
+  ams.graphs.clear();
   ams.K = 0;
   // edge operator B = C + w Ms (src/em_la.cc:122-128)
   ams.B.n = ams.B.m = c.ne;
@@ -191,9 +194,12 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
 
 template <typename T>
 void Ams<T>::set_columns(const std::vector<double> &col_omega, cudaStream_t s) {
+  if ((int)col_omega.size() != K) graphs.clear();
   K = (int)col_omega.size();
   h_omega = col_omega;
+  const double *om_before = omega.p;
   omega.upload(col_omega, s);
+  if (omega.p != om_before) graphs.clear();
   std::vector<double> distinct;
   if (two) {
     distinct = col_omega;
@@ -205,7 +211,9 @@ void Ams<T>::set_columns(const std::vector<double> &col_omega, cudaStream_t s) {
   std::vector<int> slot(K, 0);
   for (int c = 0; c < K; ++c)
     slot[c] = two ? (int)(std::lower_bound(distinct.begin(), distinct.end(), col_omega[c]) - distinct.begin()) : 0;
+  const int *cs_before = cslot.p;
   cslot.upload(slot, s);
+  if (cslot.p != cs_before) graphs.clear();
   for (int sp = 0; sp < 4; ++sp) {
     Sub &S = sub[sp];
     if (S.cinv_w == distinct && S.cinv.p) continue;
@@ -217,7 +225,9 @@ void Ams<T>::set_columns(const std::vector<double> &col_omega, cudaStream_t s) {
       coarse_inverse(S.coarse, distinct[d], X);
       std::copy(X.begin(), X.end(), all.begin() + nc2 * d);
     }
+    const double *before = S.cinv.p;
     S.cinv.upload(all, s);
+    if (S.cinv.p != before) graphs.clear();  // captured graphs hold the old address
     S.cinv_w = distinct;
   }
   EMG_CUDA(cudaStreamSynchronize(s));
@@ -228,8 +238,10 @@ template <typename T>
 void Ams<T>::ensure_workspace(cudaStream_t s) {
   (void)s;
   if (ws_K == K) return;
+  graphs.clear();
   er.alloc((size_t)ne * K);
   ex2.alloc((size_t)ne * K);
+  ed.alloc((size_t)ne * K);
   for (int sp = 0; sp < 4; ++sp) {
     Sub &S = sub[sp];
     size_t L = S.lv.size();
@@ -237,6 +249,8 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
     wx[sp].clear();
     wr[sp].clear();
     wx2[sp].clear();
+    wd[sp].clear();
+    wd[sp].resize(L + 1);
     wb[sp].resize(L + 1);
     wx[sp].resize(L + 1);
     wr[sp].resize(L + 1);
@@ -248,6 +262,7 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
       if (l < L) {
         wr[sp][l].alloc(n);
         wx2[sp][l].alloc(n);
+        wd[sp][l].alloc(n);
       }
     }
   }
@@ -270,7 +285,12 @@ void Ams<T>::spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s) {
   a.y = y;
   a.relax_w = relax_w;
   a.mode = mode;
+  KernelProfiler &pf = profiler();
+  cudaEvent_t ev = nullptr;
+  const char *bin = sizeof(T) == 4 ? "spmm_edge_fp32" : "spmm_edge_fp64";
+  if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(ne, nnzB, K, sizeof(T), two, mode), &ev);
   spmm_nnz<T>(K, a, nnzB, s);
+  if (pf.enabled) pf.end(bin, s, ev);
 }
 
 template <typename T>
@@ -290,7 +310,76 @@ static void level_spmm(const DCsr<T> &A, long nnz, int K, int mode, const double
   a.y = y;
   a.relax_w = w;
   a.mode = mode;
+  KernelProfiler &pf = profiler();
+  cudaEvent_t ev = nullptr;
+  const char *bin = sizeof(T) == 4 ? "spmm_nodal_fp32" : "spmm_nodal_fp64";
+  if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(A.n, nnz, K, sizeof(T), A.vm.p != nullptr, mode), &ev);
   spmm_nnz<T>(K, a, nnz, s);
+  if (pf.enabled) pf.end(bin, s, ev);
+}
+
+// Chebyshev coefficients for degree 2 on D^-1 A with D the l1 row sums:
+// the spectrum lies in (0, 1], smoothed interval [1/30, 1]
+struct Cheb2 {
+  double inv_theta, c1, c2;
+  Cheb2() {
+    const double lmax = 1.0, lmin = lmax / 30.0;
+    const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), s1 = th / de;
+    const double r0 = 1.0 / s1, r1 = 1.0 / (2.0 * s1 - r0);
+    inv_theta = 1.0 / th;
+    c1 = r1 * r0;
+    c2 = 2.0 * r1 / de;
+  }
+};
+
+template <typename T>
+T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b, T *rbuf, T *dbuf,
+                  bool zero_guess, const char *bin, cudaStream_t s) {
+  const bool edge = A == nullptr;
+  const T *l1c = edge ? B.l1c.p : A->l1c.p;
+  const T *l1m = edge ? (two ? B.l1m.p : nullptr) : A->l1m.p;
+  auto run = [&](int mode, const T *x, const T *bb, T *y, T *r, T *d, double c1, double c2) {
+    SpmmArgs a;
+    a.n = n;
+    a.rp = edge ? brp : A->rp.p;
+    a.ci = edge ? bci : A->ci.p;
+    a.vc = edge ? (const void *)B.vc.p : (const void *)A->vc.p;
+    a.vm = edge ? (two ? (const void *)B.vm.p : nullptr) : (const void *)A->vm.p;
+    a.l1c = l1c;
+    a.l1m = l1m;
+    a.omega = omega.p;
+    a.x = x;
+    a.b = bb;
+    a.y = y;
+    a.relax_w = relax_w;
+    a.mode = mode;
+    a.r = r;
+    a.d = d;
+    a.c1 = c1;
+    a.c2 = c2;
+    KernelProfiler &pf = profiler();
+    cudaEvent_t ev = nullptr;
+    if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(n, nnz, K, sizeof(T), a.vm != nullptr, mode), &ev);
+    spmm_nnz<T>(K, a, nnz, s);
+    if (pf.enabled) pf.end(bin, s, ev);
+  };
+  if (!cheb) {
+    if (zero_guess) {
+      jacobi0<T>(n, K, b, l1c, l1m, omega.p, relax_w, cur, s);
+      return cur;
+    }
+    run(SPMM_JAC, cur, b, oth, nullptr, nullptr, 0, 0);
+    return oth;
+  }
+  static const Cheb2 ch;
+  if (zero_guess) {
+    jacobi0_2<T>(n, K, b, l1c, l1m, omega.p, ch.inv_theta, cur, dbuf, s);
+    run(SPMM_CHEB2, dbuf, nullptr, cur, const_cast<T *>(b), nullptr, ch.c1, ch.c2);
+    return cur;
+  }
+  run(SPMM_CHEB1, cur, b, oth, rbuf, dbuf, ch.inv_theta, 0);
+  run(SPMM_CHEB2, dbuf, nullptr, oth, rbuf, nullptr, ch.c1, ch.c2);
+  return oth;
 }
 
 template <typename T>
@@ -303,49 +392,87 @@ void Ams<T>::vcycle(int sp, int l, cudaStream_t s) {
   }
   Level &lv = S.lv[l];
   const int n = lv.A.n;
-  // total Jacobi sweeps writing out of place after the zero-guess sweep:
+  const char *bin = sizeof(T) == 4 ? "spmm_nodal_fp32" : "spmm_nodal_fp64";
+  // out-of-place smoothing applications after the zero-guess one:
   // (amg_relax_times - 1) pre + amg_relax_times post; start in the buffer
-  // that makes the last sweep land in wx
+  // that makes the last one land in wx
   const int swaps = 2 * amg_relax_times - 1;
   T *cur = (swaps & 1) ? wx2[sp][l].p : wx[sp][l].p;
   T *oth = (swaps & 1) ? wx[sp][l].p : wx2[sp][l].p;
   const T *b = wb[sp][l].p;
-  jacobi0<T>(n, K, b, lv.A.l1c.p, lv.A.l1m.p, omega.p, relax_w, cur, s);
-  for (int it = 1; it < amg_relax_times; ++it) {
-    level_spmm<T>(lv.A, lv.nnzA, K, SPMM_JAC, omega.p, relax_w, cur, b, oth, s);
-    std::swap(cur, oth);
+  T *r = wr[sp][l].p, *d = wd[sp][l].p;
+  for (int it = 0; it < amg_relax_times; ++it) {
+    T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, it == 0, bin, s);
+    if (res != cur) std::swap(cur, oth);
   }
-  level_spmm<T>(lv.A, lv.nnzA, K, SPMM_RES, omega.p, relax_w, cur, b, wr[sp][l].p, s);
-  level_spmm<T>(lv.R, lv.nnzR, K, SPMM_AX, nullptr, 1.0, wr[sp][l].p, nullptr, wb[sp][l + 1].p, s);
+  level_spmm<T>(lv.A, lv.nnzA, K, SPMM_RES, omega.p, relax_w, cur, b, r, s);
+  level_spmm<T>(lv.R, lv.nnzR, K, SPMM_AX, nullptr, 1.0, r, nullptr, wb[sp][l + 1].p, s);
   vcycle(sp, l + 1, s);
   level_spmm<T>(lv.P, lv.nnzP, K, SPMM_ADD, nullptr, 1.0, wx[sp][l + 1].p, nullptr, cur, s);
   for (int it = 0; it < amg_relax_times; ++it) {
-    level_spmm<T>(lv.A, lv.nnzA, K, SPMM_JAC, omega.p, relax_w, cur, b, oth, s);
-    std::swap(cur, oth);
+    T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, false, bin, s);
+    if (res != cur) std::swap(cur, oth);
   }
 }
 
+// One AMS application.  With graphs enabled the first call for a (b, x) pair
+// runs eagerly (it also lets the SpMM autotuner pick lane layouts); the
+// second is captured into a CUDA graph that every later call replays, so the
+// few hundred small launches of the nodal V-cycles cost one graph launch.
 template <typename T>
 void Ams<T>::apply(const T *b, T *x, cudaStream_t s) {
-  // count out-of-place edge smoothing sweeps to choose the starting buffer
-  int sweeps = 0, zeros = 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  EMG_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (!use_graphs || cs != cudaStreamCaptureStatusNone || profiler().enabled) {
+    apply_eager(b, x, s);
+    return;
+  }
+  auto key = std::make_pair((const void *)b, (void *)x);
+  auto it = graphs.exec.find(key);
+  if (it != graphs.exec.end()) {
+    EMG_CUDA(cudaGraphLaunch(it->second, s));
+    return;
+  }
+  if (graphs.seen[key]++ == 0) {
+    apply_eager(b, x, s);
+    return;
+  }
+  cudaGraph_t g;
+  EMG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    apply_eager(b, x, s);
+  } catch (...) {
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  EMG_CUDA(cudaStreamEndCapture(s, &g));
+  cudaGraphExec_t ex;
+  cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  EMG_CUDA(e);
+  graphs.exec[key] = ex;
+  EMG_CUDA(cudaGraphLaunch(ex, s));
+}
+
+template <typename T>
+void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
+  // count out-of-place edge smoothing applications to choose the start buffer
+  int zeros = 0;
   for (char ch : cycle)
     if (ch == '0') ++zeros;
-  bool starts_with_smoother = !cycle.empty() && cycle[0] == '0';
-  sweeps = zeros * relax_times - (starts_with_smoother ? 1 : 0);
+  const bool starts_with_smoother = !cycle.empty() && cycle[0] == '0';
+  const int sweeps = zeros * relax_times - (starts_with_smoother ? 1 : 0);
   T *cur = (sweeps & 1) ? ex2.p : x;
   T *oth = (sweeps & 1) ? x : ex2.p;
+  const char *bin = sizeof(T) == 4 ? "spmm_edge_fp32" : "spmm_edge_fp64";
   bool zero = true;
   for (char ch : cycle) {
     if (ch == '0') {
       for (int it = 0; it < relax_times; ++it) {
-        if (zero) {
-          jacobi0<T>(ne, K, b, B.l1c.p, two ? B.l1m.p : nullptr, omega.p, relax_w, cur, s);
-          zero = false;
-        } else {
-          spmm_B(SPMM_JAC, cur, b, oth, s);
-          std::swap(cur, oth);
-        }
+        T *res = smooth(nullptr, nnzB, ne, cur, oth, b, er.p, ed.p, zero, bin, s);
+        if (res != cur) std::swap(cur, oth);
+        zero = false;
       }
       continue;
     }

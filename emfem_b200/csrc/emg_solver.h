@@ -2,6 +2,8 @@
 #pragma once
 
 #include <functional>
+#include <map>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -10,6 +12,31 @@
 #include "emg_linalg.h"
 
 namespace emg {
+
+// Cache of instantiated CUDA graphs keyed by an argument pair; owns the execs.
+struct GraphCache {
+  std::map<std::pair<const void *, void *>, cudaGraphExec_t> exec;
+  std::map<std::pair<const void *, void *>, int> seen;
+  GraphCache() = default;
+  GraphCache(const GraphCache &) = delete;
+  GraphCache &operator=(const GraphCache &) = delete;
+  GraphCache(GraphCache &&o) noexcept : exec(std::move(o.exec)), seen(std::move(o.seen)) { o.exec.clear(); }
+  GraphCache &operator=(GraphCache &&o) noexcept {
+    if (this != &o) {
+      clear();
+      exec = std::move(o.exec);
+      seen = std::move(o.seen);
+      o.exec.clear();
+    }
+    return *this;
+  }
+  ~GraphCache() { clear(); }
+  void clear() {
+    for (auto &kv : exec) cudaGraphExecDestroy(kv.second);
+    exec.clear();
+    seen.clear();
+  }
+};
 
 // AMS (Hiptmair-Xu auxiliary space preconditioner, as hypre's AMS applies it)
 // for B(w) = C + w Ms on K real columns with per-column w.
@@ -38,21 +65,29 @@ struct Ams {
   int relax_times = 1;
   double relax_w = 1.0;
   int amg_relax_times = 1;
+  int cheb = 1;                    // 1: degree-2 Chebyshev smoothing, 0: l1-Jacobi
+  bool use_graphs = true;          // replay each application as one CUDA graph
+  GraphCache graphs;
   // per-call state
   int K = 0;
   DBuf<double> omega;              // K
   DBuf<int> cslot;                 // K, coarse-inverse index per column
   std::vector<double> h_omega;
   // workspace
-  DBuf<T> er, ex2;
-  std::vector<DBuf<T>> wb[4], wx[4], wr[4], wx2[4];
+  DBuf<T> er, ex2, ed;
+  std::vector<DBuf<T>> wb[4], wx[4], wr[4], wx2[4], wd[4];
 
   void set_columns(const std::vector<double> &col_omega, cudaStream_t s);
   void apply(const T *b, T *x, cudaStream_t s);
+  void apply_eager(const T *b, T *x, cudaStream_t s);
   void spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s);
   size_t device_bytes() const;
 
   void vcycle(int sp, int l, cudaStream_t s);
+  // one smoothing application on operator A (edge B when A == nullptr);
+  // returns the buffer holding the result (cur, or oth after a swap)
+  T *smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b, T *rbuf, T *dbuf, bool zero_guess,
+            const char *bin, cudaStream_t s);
   void ensure_workspace(cudaStream_t s);
   int ws_K = 0;
 };

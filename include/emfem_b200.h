@@ -176,6 +176,13 @@ int emg_solve_block(emg_context *ctx, int k, const double *freqs, const double *
 int emg_solve_block_dev(emg_context *ctx, int k, const double *freqs, const double *rhs_dev, double *x_dev,
                         const emg_block_opts *opts, emg_solve_info *infos);
 
+/* Batched MT right-hand sides (assemble_rhs_mt, src/em_fwd.cc:488-580, for k
+ * columns at once): column j is polarisation modes[j] (EMG_SOL_MT_XY/YX) at
+ * frequency freqs[j]; boundary values from the layered plane waves, lifting
+ * on the device.  s: n x k complex, interleaved (host or device pointer). */
+int emg_assemble_rhs_mt_block(emg_context *ctx, int k, const double *freqs, const int *modes, double *s);
+int emg_assemble_rhs_mt_block_dev(emg_context *ctx, int k, const double *freqs, const int *modes, double *s_dev);
+
 /* ---- kernel-level entry points on device pointers (tests, benchmarks) -- */
 /* y = (C + i w Ms) x  (conj_out=0)  or its conjugate (conj_out=1, the
  * real-form operator of matshell_mult_a) for k complex columns. */
@@ -184,6 +191,13 @@ int emg_spmv_complex_dev(emg_context *ctx, int k, const double *omegas_host, con
 /* per-kernel device timing of the last call of each kind (ms) */
 int emg_last_kernel_ms(emg_context *ctx, const char *name, double *ms);
 int emg_stream_synchronize(emg_context *ctx);
+/* number of kernels this library has launched in the process */
+int emg_launch_count(long *n);
+/* per-kernel event profiler (bins "spmm_edge_fp32", "spmm_edge_fp64",
+ * "spmm_nodal_fp32", "spmm_nodal_fp64"): launches, device ms and algorithmic
+ * bytes accumulated since emg_profile_enable(1) */
+int emg_profile_enable(int on);
+int emg_profile_get(const char *bin, long *count, double *ms, double *bytes);
 
 #ifdef __cplusplus
 }

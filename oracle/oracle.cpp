@@ -32,6 +32,11 @@
 
 typedef std::complex<double> cplx;
 
+#include <chrono>
+static double wall() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 static const double PI = 3.14159265358979323846;   // em_defs.h:16
 static const double MU = 4 * PI * 1E-7;            // em_defs.h:17
 static const double DTOR = PI / 180.0;             // em_defs.h:21
@@ -1394,7 +1399,9 @@ int orc_solve(const OrcMesh *m, int n, const int *rp, const int *ci, const doubl
   s.M.v.assign(M, M + rp[n]);
   s.B = s.C;  // create_pc (em_la.cc:122-128): B = C + M
   for (size_t k = 0; k < s.B.v.size(); ++k) s.B.v[k] += M[k];
+  double t0 = wall();
   ams_setup(s.ams, m, s.B);
+  double t1 = wall();
   std::vector<double> b(2 * n), x(2 * n);
   std::copy(s_re, s_re + n, b.begin());
   std::copy(s_im, s_im + n, b.begin() + n);
@@ -1405,6 +1412,8 @@ int orc_solve(const OrcMesh *m, int n, const int *rp, const int *ci, const doubl
   if (stats) {
     stats[0] = tr;
     stats[1] = (double)s.inner_its;
+    stats[2] = t1 - t0;       // AMS setup seconds
+    stats[3] = wall() - t1;   // FGMRES seconds
   }
   return its;
 }
