@@ -41,6 +41,13 @@ METRIC = "RHS solved/s at 1e-8 residual: mixed+batched+warm-start vs plain FP64 
 UNIT = "RHS/s"
 
 
+def log(msg):
+    print("[bench %.0fs] %s" % (time.perf_counter() - _T0, msg), file=sys.stderr, flush=True)
+
+
+_T0 = time.perf_counter()
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -283,18 +290,22 @@ def ours(args):
         infos_last = ctx.solve_block_dev(colf, rhs.data_ptr(), x.data_ptr(), rtol=1e-8, max_it=200,
                                          inner_fp32=True)
         t3 = time.perf_counter()
-        for k, v in (("assemble", t1 - t0), ("rhs", t2 - t1), ("setup+solve", t3 - t2)):
+        su = ctx.last_kernel_ms("block_setup") / 1e3
+        for k, v in (("assemble", t1 - t0), ("rhs", t2 - t1), ("ams_setup", su), ("solve", t3 - t2 - su)):
             breakdown[k] = breakdown.get(k, 0.0) + v
 
-    for _ in range(args.warmup):
+    log("problem %s: %d tets, %d edges; warm-up %d steps" % (prob.name, prob.mesh.n_tets, ne, args.warmup))
+    for i in range(args.warmup):
         step()
+        log("warm-up step %d: %s outer its %s" % (i, {k: round(v, 2) for k, v in breakdown.items()},
+                                                  [inf.outer_its for inf in infos_last]))
     breakdown.clear()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
+    log("timed region: %d steps" % args.steps)
     clocks = Clocks(local)
     clocks.start()
-    E.profile_enable(True)
     l0 = E.launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -312,11 +323,20 @@ def ours(args):
     barrier(world)
     ms_step = ms / args.steps
     value = world * K * args.steps / (ms / 1e3)
+    log("timed: %.1f ms/step" % ms_step)
+    # kernel attribution: one more step with the event profiler on (it runs
+    # the AMS launch by launch, so it stays out of the timed region)
+    E.profile_enable(True)
+    tp0 = time.perf_counter()
+    step()
+    torch.cuda.synchronize()
+    prof_step_s = time.perf_counter() - tp0
     bins = {}
-    for b in ("spmm_edge_fp32", "spmm_edge_fp64", "spmm_nodal_fp32"):
+    for b in ("spmm_edge_fp32", "spmm_edge_fp64", "spmm_nodal_fp32", "spmm_nodal_fp64"):
         n, t, by = E.profile_get(b)
         bins[b] = (n, t, by)
     E.profile_enable(False)
+    log("profiled step: %.1f s" % prof_step_s)
     conv = [(i.true_rel_res, i.outer_its) for i in infos_last]
     all_conv = all(i.reason == 0 and i.true_rel_res <= 1e-8 for i in infos_last)
     dom = max(bins, key=lambda b: bins[b][1])
@@ -328,10 +348,13 @@ def ours(args):
             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
             "algorithmic_bytes_per_launch": b_l / max(n_l, 1), "launches": n_l,
             "avg_launch_us": 1e3 * t_l / max(n_l, 1),
-            "share_of_step": t_l / ms if ms > 0 else None}
+            "measured": "CUDA events around every launch of the kernel during one profiled step of this "
+                        "workload (launch by launch) right after the timed region",
+            "share_of_profiled_step": t_l / (prof_step_s * 1e3) if prof_step_s > 0 else None}
 
     # ---- e2e through the host-buffer C ABI ----------------------------------
     e2e = None
+    log("e2e")
     if not args.no_e2e:
         h_x = np.zeros((ne, K), dtype=np.complex128)
         torch.cuda.synchronize()
@@ -350,6 +373,7 @@ def ours(args):
 
     # ---- plain FP64 drop-in on a subset of the columns ----------------------
     plain = None
+    log("plain FP64 path")
     if args.plain_freqs > 0:
         idx = np.unique(np.linspace(0, freqs.size - 1, args.plain_freqs).round().astype(int))
         torch.cuda.synchronize()
@@ -372,6 +396,7 @@ def ours(args):
 
     # ---- CPU baseline --------------------------------------------------------
     cpu = None
+    log("cpu baseline")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             s = cpu_sample(prob)

@@ -462,4 +462,112 @@ void assemble_nodal(Context &c, HCsr out[4]) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// G^T B as a vertex x edge operator.  The gradient-space residual of AMS,
+// G^T (b - B x), is formed as G^T b - (G^T B) x: G^T C vanishes exactly on
+// every element without a boundary edge (curl grad = 0), so the product keeps
+// no trace of the curl-curl scale that swamps w sigma Ms in the air when
+// B x is evaluated in FP32.
+// ---------------------------------------------------------------------------
+void build_gtb_pattern(Context &c) {
+  const int nv = c.nv, nt = c.nt;
+  std::vector<int> v2t_rp(nv + 1, 0), v2t;
+  for (int t = 0; t < nt; ++t)
+    for (int i = 0; i < 4; ++i) v2t_rp[c.h_tets[4 * (size_t)t + i] + 1]++;
+  for (int v = 0; v < nv; ++v) v2t_rp[v + 1] += v2t_rp[v];
+  v2t.resize(v2t_rp[nv]);
+  {
+    std::vector<int> pos(v2t_rp.begin(), v2t_rp.end() - 1);
+    for (int t = 0; t < nt; ++t)
+      for (int i = 0; i < 4; ++i) v2t[pos[c.h_tets[4 * (size_t)t + i]]++] = t;
+  }
+  std::vector<int> cnt(nv + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<int> buf;
+#pragma omp for schedule(dynamic, 4096)
+    for (int v = 0; v < nv; ++v) {
+      buf.clear();
+      for (int k = v2t_rp[v]; k < v2t_rp[v + 1]; ++k)
+        for (int i = 0; i < 6; ++i) buf.push_back(c.h_t2e[6 * (size_t)v2t[k] + i]);
+      std::sort(buf.begin(), buf.end());
+      cnt[v + 1] = (int)(std::unique(buf.begin(), buf.end()) - buf.begin());
+    }
+  }
+  c.h_grp.assign(nv + 1, 0);
+  for (int v = 0; v < nv; ++v) c.h_grp[v + 1] = c.h_grp[v] + cnt[v + 1];
+  c.h_gci.resize(c.h_grp[nv]);
+#pragma omp parallel
+  {
+    std::vector<int> buf;
+#pragma omp for schedule(dynamic, 4096)
+    for (int v = 0; v < nv; ++v) {
+      buf.clear();
+      for (int k = v2t_rp[v]; k < v2t_rp[v + 1]; ++k)
+        for (int i = 0; i < 6; ++i) buf.push_back(c.h_t2e[6 * (size_t)v2t[k] + i]);
+      std::sort(buf.begin(), buf.end());
+      int u = (int)(std::unique(buf.begin(), buf.end()) - buf.begin());
+      std::copy(buf.begin(), buf.begin() + u, c.h_gci.begin() + c.h_grp[v]);
+    }
+  }
+  c.grp.upload(c.h_grp, c.stream);
+  c.gci.upload(c.h_gci, c.stream);
+}
+
+// gslot[t*24 + p*6 + k] = slot of (ctet[t][p], cedge[t][k]) in the G^T B pattern
+__global__ void gslot_map_kernel(int nt, const int *__restrict__ ctet, const int *__restrict__ cedge,
+                                 const int *__restrict__ rp, const int *__restrict__ ci, int *__restrict__ slot) {
+  long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)nt * 24) return;
+  int t = (int)(idx / 24), ent = (int)(idx % 24);
+  int row = __ldg(ctet + 4 * (long)t + ent / 6), col = __ldg(cedge + 6 * (long)t + ent % 6);
+  slot[idx] = find_col(ci, __ldg(rp + row), __ldg(rp + row + 1), col);
+}
+
+__global__ void __launch_bounds__(128) assemble_gtb_kernel(ElemIn in, int nt, const int *__restrict__ gslot,
+                                                            double *__restrict__ gc, double *__restrict__ gm) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  double c[36], m[36];
+  TetGeom g;
+  const bool touches_bdr = element_matrices(in, t, c, m, g);
+  // (G_e^T K)[p][k] = sum over local edges j=(a,b): (-1 if p==a, +1 if p==b) K[j][k]
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double vm = 0, vc = 0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const double sgn = (kEdgeP(j) == p) ? -1.0 : ((kEdgeQ(j) == p) ? 1.0 : 0.0);
+        if (sgn != 0.0) {
+          vm += sgn * m[j * 6 + k];
+          vc += sgn * c[j * 6 + k];
+        }
+      }
+      const int sl = __ldg(gslot + 24 * (long)t + p * 6 + k);
+      atomicAdd(gm + sl, vm);
+      if (touches_bdr) atomicAdd(gc + sl, vc);
+    }
+  }
+}
+
+void assemble_gtb(Context &c, DBuf<double> &gc, DBuf<double> &gm) {
+  if (c.h_grp.empty()) build_gtb_pattern(c);
+  if (!c.gslot.p) {
+    c.gslot.alloc((size_t)c.nt * 24);
+    long n24 = (long)c.nt * 24;
+    gslot_map_kernel<<<(unsigned)((n24 + 255) / 256), 256, 0, c.stream>>>(c.nt, c.ctet.p, c.cedge.p, c.grp.p, c.gci.p,
+                                                                          c.gslot.p);
+    EMG_LAUNCH_CHECK();
+  }
+  long nnz = c.h_grp[c.nv];
+  gc.alloc(nnz);
+  gm.alloc(nnz);
+  gc.zero(c.stream);
+  gm.zero(c.stream);
+  assemble_gtb_kernel<<<(unsigned)((c.nt + 127) / 128), 128, 0, c.stream>>>(elem_in(c), c.nt, c.gslot.p, gc.p, gm.p);
+  EMG_LAUNCH_CHECK();
+}
+
 }  // namespace emg

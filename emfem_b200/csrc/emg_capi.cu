@@ -13,6 +13,7 @@
 #include <string>
 #include <array>
 #include <atomic>
+#include <chrono>
 
 #include "emg_internal.h"
 #include "emg_kernels.cuh"
@@ -206,6 +207,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_amg_relax_times") o.amg_relax_times = geti(k, v);
     else if (key == "emg_amg_pmax") o.amg_pmax = geti(k, v);
     else if (key == "emg_smoother") o.smoother_cheb = elist(k, v, {"l1jacobi", "chebyshev"});
+    else if (key == "emg_fp32_cycle") o.fp32_cycle = v;
     else if (key == "emg_graphs") o.graphs = v.empty() ? 1 : getb(v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
     else if (key.rfind("A_", 0) == 0 || key.rfind("B_", 0) == 0) ignored.push_back(k);
@@ -590,6 +592,8 @@ int emg_create_linear_system(emg_context *c, int tidx) {
   build_sparsity(*c);
   build_vertex_pattern(*c);
   build_slot_maps(*c);
+  c->gslot.release();
+  build_gtb_pattern(*c);
   c->have_ls = true;
   c->assembled = false;
   c->have_pc = false;
@@ -1082,6 +1086,7 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
   }
   const double wref = std::exp(lg / k);
   const bool fp32 = o.inner_fp32 != 0;
+  auto t0 = std::chrono::steady_clock::now();
   if (fp32 && !w.block_ready32) {
     ams_setup<float>(c, w.bams32, false, 0.0, wref);
     w.block_ready32 = true;
@@ -1090,6 +1095,7 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     ams_setup<double>(c, w.bams64, false, 0.0, wref);
     w.block_ready64 = true;
   }
+  c.kernel_ms["block_setup"] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (fp32) w.bams32.set_columns(col, c.stream);
   else w.bams64.set_columns(col, c.stream);
   // b = conj(s): the real-form system equals (C + i w Ms) z = conj(s)
@@ -1137,7 +1143,7 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
   auto pc32 = [&](const double *r_, double *z_) {
     cvt_d2f((long)n * K2, r_, w.f_in.p, c.stream);
     w.bams32.apply(w.f_in.p, w.f_out.p, c.stream);
-    cvt_f2d((long)n * K2, w.f_out.p, z_, c.stream);
+    add_gradient_f2d(n, K2, c.edges.p, w.f_out.p, w.bams32.gphi(), z_, c.stream);
   };
   auto pc = [&](const double *v, double *z) {
     if (fp32) w.fcg64.solve_with(n, K2, pc32, opB64, v, z, c.opt.inner_rtol, c.opt.inner_max_it, c.stream);

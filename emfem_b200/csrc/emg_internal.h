@@ -143,6 +143,7 @@ struct Options {
   int inner_max_it = 100;
   int fcg_mmax = 1;
   std::string ams_cycle = "034515430";  // cycle type 13
+  std::string fp32_cycle = "034501";    // cycle of the FP32 AMS (gradient last)
   int ams_relax_times = 1;
   double ams_relax_weight = 1.0;
   double amg_theta = 0.25;
@@ -201,6 +202,9 @@ struct Context {
   std::vector<int> h_vrp, h_vci;
   DBuf<int> vrp, vci, vslot;       // vslot: 16 per tet
   DBuf<int> vinc_rp, vinc;         // vertex -> incident edge (e*2+endpoint)
+  // vertex x edge pattern of G^T B (row v: edges of the tets around v)
+  std::vector<int> h_grp, h_gci;
+  DBuf<int> grp, gci, gslot;       // gslot: 24 per tet (4 vertices x 6 edges)
   // AMS (the preconditioner objects live in the workspace)
   bool have_pc = false;
   double pc_omega = 0;             // omega the hierarchy was built for (plain path)
@@ -221,6 +225,8 @@ void canonicalize(Context &c);            // device: sorted tets + canonical edg
 void build_slot_maps(Context &c);         // device: tet -> CSR slots
 void assemble_edge(Context &c);           // device: C, Ms, bdr cells
 void assemble_nodal(Context &c, HCsr out[4]);  // device + download (G, Pi_x, Pi_y, Pi_z)
+void build_gtb_pattern(Context &c);       // host pattern + device slot map of G^T B
+void assemble_gtb(Context &c, DBuf<double> &gc, DBuf<double> &gm);  // G^T C (boundary part), G^T Ms
 void create_pc(Context &c, bool per_frequency_hierarchy, const std::vector<double> &omegas);
 void destroy_pc(Context &c);
 

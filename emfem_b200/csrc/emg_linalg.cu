@@ -347,6 +347,23 @@ void cvt_f2d(long count, const float *a, double *b, cudaStream_t s) {
   cvt_f2d_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(count, a, b);
   EMG_LAUNCH_CHECK();
 }
+__global__ void add_gradient_f2d_kernel(long total, int K, const int *__restrict__ edges, const float *__restrict__ x,
+                                        const float *__restrict__ phi, double *__restrict__ z) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  long e = i / K;
+  int c = (int)(i % K);
+  int v0 = __ldg(edges + 2 * e), v1 = __ldg(edges + 2 * e + 1);
+  z[i] = (double)x[i] + ((double)__ldg(phi + (long)v1 * K + c) - (double)__ldg(phi + (long)v0 * K + c));
+}
+
+void add_gradient_f2d(int ne, int K, const int *edges, const float *x, const float *phi, double *z, cudaStream_t s) {
+  long total = (long)ne * K;
+  if (!total) return;
+  add_gradient_f2d_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, edges, x, phi, z);
+  EMG_LAUNCH_CHECK();
+}
+
 template <typename T>
 void fill_zero(long count, T *a, cudaStream_t s) {
   if (count) EMG_CUDA(cudaMemsetAsync(a, 0, count * sizeof(T), s));

@@ -56,6 +56,8 @@ void jacobi0_2(int n, int K, const T *b, const T *l1c, const T *l1m, const doubl
 // precision conversion of block vectors
 void cvt_d2f(long count, const double *a, float *b, cudaStream_t s);
 void cvt_f2d(long count, const float *a, double *b, cudaStream_t s);
+// z = x + G phi in FP64 (edge e: phi[v1] - phi[v0]) for K columns
+void add_gradient_f2d(int ne, int K, const int *edges, const float *x, const float *phi, double *z, cudaStream_t s);
 template <typename T>
 void fill_zero(long count, T *a, cudaStream_t s);
 

@@ -111,6 +111,16 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   ams.cheb = c.opt.smoother_cheb;
   ams.two = !per_frequency;
   ams.use_graphs = c.opt.graphs != 0;
+  // FP32 applications close with the gradient correction and hand it back
+  // as a potential: after it, no FP32 product touches the (air) gradient
+  // component, which can exceed the rest of the iterate by 1e10 at low
+  // frequency, far beyond what FP32 rounding of C x tolerates
+  ams.split_gradient = sizeof(T) == 4;
+  if (ams.split_gradient) {
+    ams.cycle = c.opt.fp32_cycle;
+    if (ams.cycle.empty() || ams.cycle.back() != '1')
+      fail(EMG_ERR_OPTION, "the FP32 AMS cycle must end with the gradient correction '1'");
+  }
   ams.graphs.clear();
   ams.K = 0;
   // edge operator B = C + w Ms (src/em_la.cc:122-128)
@@ -143,6 +153,26 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
       for (int d = 0; d < 3; ++d)
         tg[3 * (size_t)e + d] = (T)(c.h_pts[3 * (size_t)c.h_edges[2 * e + 1] + d] - c.h_pts[3 * (size_t)c.h_edges[2 * e] + d]);
     ams.tangent.upload(tg, s);
+    EMG_CUDA(cudaStreamSynchronize(s));
+  }
+  // G^T B for the gradient-space residual
+  {
+    DBuf<double> gc, gm;
+    assemble_gtb(c, gc, gm);
+    ams.grp = c.grp.p;
+    ams.gci = c.gci.p;
+    ams.nnzG = c.h_grp[c.nv];
+    unsigned gg = (unsigned)((ams.nnzG + 255) / 256);
+    ams.gvc.alloc(ams.nnzG);
+    if (per_frequency) {
+      combine_kernel<T><<<gg, 256, 0, s>>>(ams.nnzG, gc.p, gm.p, w, ams.gvc.p);
+      ams.gvm.release();
+    } else {
+      ams.gvm.alloc(ams.nnzG);
+      combine_kernel<T><<<gg, 256, 0, s>>>(ams.nnzG, gc.p, nullptr, 0.0, ams.gvc.p);
+      combine_kernel<T><<<gg, 256, 0, s>>>(ams.nnzG, gm.p, nullptr, 0.0, ams.gvm.p);
+    }
+    EMG_LAUNCH_CHECK();
     EMG_CUDA(cudaStreamSynchronize(s));
   }
   // nodal subspace operators and their hierarchies
@@ -242,6 +272,7 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
   er.alloc((size_t)ne * K);
   ex2.alloc((size_t)ne * K);
   ed.alloc((size_t)ne * K);
+  gtmp.alloc((size_t)nv * K);
   for (int sp = 0; sp < 4; ++sp) {
     Sub &S = sub[sp];
     size_t L = S.lv.size();
@@ -467,7 +498,8 @@ void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
   T *oth = (sweeps & 1) ? x : ex2.p;
   const char *bin = sizeof(T) == 4 ? "spmm_edge_fp32" : "spmm_edge_fp64";
   bool zero = true;
-  for (char ch : cycle) {
+  for (size_t ci = 0; ci < cycle.size(); ++ci) {
+    const char ch = cycle[ci];
     if (ch == '0') {
       for (int it = 0; it < relax_times; ++it) {
         T *res = smooth(nullptr, nnzB, ne, cur, oth, b, er.p, ed.p, zero, bin, s);
@@ -478,16 +510,46 @@ void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
     }
     int sp = ch == '1' ? 0 : (ch - '2');
     if (sp < 0 || sp > 3) fail(EMG_ERR_OPTION, "bad AMS cycle character '%c'", ch);
-    if (zero) {
-      fill_zero<T>((long)ne * K, cur, s);
-      EMG_CUDA(cudaMemcpyAsync(er.p, b, sizeof(T) * (size_t)ne * K, cudaMemcpyDeviceToDevice, s));
-      zero = false;
-    } else {
-      spmm_B(SPMM_RES, cur, b, er.p, s);
-    }
     const T *tg = sp == 0 ? nullptr : tangent.p;
-    ams_restrict<T>(nv, K, sp, inc_rp, inc, tg, er.p, wb[sp][0].p, s);
+    if (sp == 0) {
+      // gradient space: G^T (b - B x) = G^T b - (G^T B) x
+      if (zero) {
+        fill_zero<T>((long)ne * K, cur, s);
+        ams_restrict<T>(nv, K, 0, inc_rp, inc, nullptr, b, wb[0][0].p, s);
+        zero = false;
+      } else {
+        ams_restrict<T>(nv, K, 0, inc_rp, inc, nullptr, b, gtmp.p, s);
+        SpmmArgs a;
+        a.n = nv;
+        a.rp = grp;
+        a.ci = gci;
+        a.vc = gvc.p;
+        a.vm = two ? (const void *)gvm.p : nullptr;
+        a.l1c = a.l1m = nullptr;
+        a.omega = omega.p;
+        a.x = cur;
+        a.b = gtmp.p;
+        a.y = wb[0][0].p;
+        a.relax_w = 1.0;
+        a.mode = SPMM_RES;
+        a.r = a.d = nullptr;
+        a.c1 = a.c2 = 0;
+        spmm_nnz<T>(K, a, nnzG, s);
+      }
+    } else {
+      if (zero) {
+        fill_zero<T>((long)ne * K, cur, s);
+        EMG_CUDA(cudaMemcpyAsync(er.p, b, sizeof(T) * (size_t)ne * K, cudaMemcpyDeviceToDevice, s));
+        zero = false;
+      } else {
+        spmm_B(SPMM_RES, cur, b, er.p, s);
+      }
+      ams_restrict<T>(nv, K, sp, inc_rp, inc, tg, er.p, wb[sp][0].p, s);
+    }
     vcycle(sp, 0, s);
+    // split form: the closing gradient correction stays a vertex potential
+    // (wx[0][0]); the caller adds G phi in higher precision
+    if (split_gradient && sp == 0 && ci + 1 == cycle.size()) continue;
     ams_prolong_add<T>(ne, K, sp, edges, tg, wx[sp][0].p, cur, s);
   }
   if (cur != x) EMG_CUDA(cudaMemcpyAsync(x, cur, sizeof(T) * (size_t)ne * K, cudaMemcpyDeviceToDevice, s));

@@ -59,6 +59,11 @@ struct Ams {
   bool two = true;  // two value parts (batched) or combined (one frequency)
   Sub sub[4];
   DBuf<T> tangent;
+  // G^T B (vertex x edge): curl part (boundary elements only) and mass part
+  const int *grp = nullptr, *gci = nullptr;
+  long nnzG = 0;
+  DBuf<T> gvc, gvm;
+  DBuf<T> gtmp;                    // G^T b (nv x K)
   int ne = 0, nv = 0;
   const int *edges = nullptr, *inc_rp = nullptr, *inc = nullptr;
   std::string cycle = "034515430";
@@ -67,6 +72,7 @@ struct Ams {
   int amg_relax_times = 1;
   int cheb = 1;                    // 1: degree-2 Chebyshev smoothing, 0: l1-Jacobi
   bool use_graphs = true;          // replay each application as one CUDA graph
+  bool split_gradient = false;     // last '1' of the cycle returned as potential gphi()
   GraphCache graphs;
   // per-call state
   int K = 0;
@@ -80,6 +86,7 @@ struct Ams {
   void set_columns(const std::vector<double> &col_omega, cudaStream_t s);
   void apply(const T *b, T *x, cudaStream_t s);
   void apply_eager(const T *b, T *x, cudaStream_t s);
+  const T *gphi() const { return wx[0][0].p; }  // gradient potential (split form)
   void spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s);
   size_t device_bytes() const;
 

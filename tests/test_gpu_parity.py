@@ -226,7 +226,13 @@ def test_block_solve_matches_plain(mt_small, fp32):
                 freqs.append(f)
                 ref.append(_direct(orp, oci, Co, Mo, sr, si))
         rhs = np.stack(cols, axis=1)
+        # the outer FP64 FGMRES sets the accuracy: at rtol 1e-8 every column
+        # meets its residual; compared with the exact discrete solution at
+        # rtol 1e-10 every DOF agrees to 1e-6 whatever the inner precision
         x, infos = c.solve_block(freqs, rhs, rtol=1e-8, max_it=200, inner_fp32=fp32)
         for j in range(len(freqs)):
             assert infos[j].reason == 0 and infos[j].true_rel_res <= 1e-8
+        x, infos = c.solve_block(freqs, rhs, rtol=1e-10, max_it=300, inner_fp32=fp32)
+        for j in range(len(freqs)):
+            assert infos[j].reason == 0 and infos[j].true_rel_res <= 1e-10
             assert np.abs(x[:, j] - ref[j]).max() / np.abs(ref[j]).max() < 1e-6
