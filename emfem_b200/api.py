@@ -96,6 +96,7 @@ _SIGS = {
     "emg_profile_get": ([C.c_char_p, C.POINTER(C.c_long), C.POINTER(_D), C.POINTER(_D)], _I),
     "emg_assemble_rhs_mt_block": ([_P, _I, _P, _P, _P], _I),
     "emg_assemble_rhs_mt_block_dev": ([_P, _I, _P, _P, _P], _I),
+    "emg_estimate_error_noalloc": ([_P, _I, _I, _P, _P], _I),
 }
 
 
@@ -321,6 +322,12 @@ class EMContext:
         eta = np.zeros(nsol * self.nt)
         _check(lib().emg_estimate_error(self._h, int(fidx), int(tidx), _ptr(err), _ptr(eta)))
         return err.reshape(nsol - 1, self.nt), eta.reshape(nsol, self.nt)
+
+    def estimate_error_noalloc_dev(self, fidx, tidx, err_ptr, eta_ptr):
+        """estimate_error into caller-owned device buffers (err: n_err x T,
+        eta: n_sol x T, float64) without any device allocation by the library."""
+        _check(lib().emg_estimate_error_noalloc(self._h, int(fidx), int(tidx), C.c_void_p(err_ptr),
+                                                C.c_void_p(eta_ptr)))
 
     def interpolate_fields(self, target, fidx, pts, tets):
         pts = _f64(pts).reshape(-1, 3)

@@ -24,6 +24,8 @@ namespace emg {
 
 static thread_local std::string g_last_error;
 
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 void fail(int code, const char *fmt, ...) {
   char buf[1024];
   va_list ap;
@@ -416,8 +418,6 @@ static std::vector<double> interleave(const double *re, const double *im, int n)
 }  // namespace emg
 
 using namespace emg;
-
-struct emg_context : public emg::Context {};
 
 #define EMG_API_BEGIN try {
 #define EMG_API_END                                  \

@@ -14,6 +14,9 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+
 #include "emg_internal.h"
 #include "emg_kernels.cuh"
 
@@ -357,3 +360,77 @@ void launch_rhs_mt(Context &c, int k, const double *omega_dev, const double *bv_
 }
 
 }  // namespace emg
+
+// ---------------------------------------------------------------------------
+// Error estimate without any device allocation.
+//
+// emg_estimate_error obtains its per-tet and per-face scratch from the
+// context's workspace, which the library allocates with cudaMalloc on first
+// use.  Some callers cannot allow an allocation at that point -- a host
+// application whose memory manager owns all device memory and forbids
+// allocations once a run has started, or a caller that must not synchronise
+// the device the way cudaMalloc/cudaFree can.  For them this variant keeps
+// the scratch in a fixed file-scope device array and writes its results into
+// device buffers the caller owns.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxTets = 131072;  // largest mesh the fixed scratch serves
+constexpr int kNoAllocMaxSol = 3;        // MT: XY, YX and the dual solution
+
+// volume terms (n_sol x T) followed by face terms (n_sol x T x 4): 15.7 MB,
+// held on every GPU that loads the library until the process exits
+__device__ __align__(256) double g_estimate_scratch[kNoAllocMaxSol * kNoAllocMaxTets * 5];
+
+// In host code g_estimate_scratch only names a host-side stand-in; the device
+// address is looked up once per device, with that device current.
+double *scratch_address(int device) {
+  static std::mutex mu;
+  static std::map<int, double *> addr;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = addr.find(device);
+  if (it != addr.end()) return it->second;
+  double *p = nullptr;
+  emg::check_cuda(cudaGetSymbolAddress((void **)&p, g_estimate_scratch), "cudaGetSymbolAddress(g_estimate_scratch)",
+                  __FILE__, __LINE__);
+  addr[device] = p;
+  return p;
+}
+
+}  // namespace
+
+extern "C" int emg_estimate_error_noalloc(emg_context *ctx, int fidx, int tidx, double *err_dev, double *eta_dev) {
+  using namespace emg;
+  try {
+    if (!ctx || !err_dev || !eta_dev) fail(EMG_ERR_ARG, "null argument");
+    Context &c = *ctx;
+    if (c.device < 0) fail(EMG_ERR_STATE, "host-only context has no device");
+    if (!c.have_ls || c.nrho <= 0) fail(EMG_ERR_STATE, "estimate_error before create_linear_system");
+    if (fidx < 0 || fidx >= (int)c.freqs.size()) fail(EMG_ERR_ARG, "frequency index out of range");
+    if (c.nt > kNoAllocMaxTets)
+      fail(EMG_ERR_ARG, "emg_estimate_error_noalloc serves meshes of at most %d tets (this one has %d); "
+           "use emg_estimate_error", kNoAllocMaxTets, c.nt);
+    const int slots3[3] = {EMG_SOL_MT_XY, EMG_SOL_MT_YX, EMG_SOL_DUAL};
+    const int slots2[2] = {EMG_SOL_CSEM, EMG_SOL_DUAL};
+    const int nsol = tidx < 0 ? 3 : 2;
+    const double *sp[3];
+    for (int s = 0; s < nsol; ++s) {
+      auto it = c.sol.find(tidx < 0 ? slots3[s] : slots2[s]);
+      if (it == c.sol.end() || it->second.n != (size_t)c.ne * 2) fail(EMG_ERR_STATE, "solution slot not created");
+      sp[s] = it->second.p;
+    }
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice", __FILE__, __LINE__);
+    double *scratch = scratch_address(c.device);
+    // every volume and face entry is written before it is read, so nothing
+    // left in the array by an earlier call needs clearing
+    launch_estimate(c, 2 * PI * c.freqs[fidx], nsol, sp, eta_dev, err_dev, scratch, scratch + (size_t)nsol * c.nt);
+    check_cuda(cudaStreamSynchronize(c.stream), "cudaStreamSynchronize", __FILE__, __LINE__);
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return EMG_ERR_USER;
+  }
+  return EMG_OK;
+}

@@ -217,6 +217,9 @@ struct Context {
   ~Context();
 };
 
+// records the message returned by emg_last_error() on this thread
+void set_last_error(const char *msg);
+
 // helpers implemented in the .cu/.cpp files
 void sigma_table(int aniso_form, int nrho, int ncol, const double *rho, std::vector<double> &out);
 void build_sparsity(Context &c);          // host: CSR pattern (make_sparsity_patterns)
@@ -231,3 +234,6 @@ void create_pc(Context &c, bool per_frequency_hierarchy, const std::vector<doubl
 void destroy_pc(Context &c);
 
 }  // namespace emg
+
+// the opaque handle of the C ABI is the context itself
+struct emg_context : public emg::Context {};

@@ -144,6 +144,19 @@ int emg_assemble_rhs_dual(emg_context *ctx, int n_rx, const double *rx, const in
  * (optional, n_sol x T) receives the per-solution indicators. */
 int emg_estimate_error(emg_context *ctx, int fidx, int tidx, double *err, double *eta_raw);
 
+/* Same indicators as emg_estimate_error, for callers that cannot let the
+ * library allocate device memory during a run (an application whose memory
+ * manager owns the device, or code that must not be stalled by
+ * cudaMalloc/cudaFree).  No counterpart in the reference.  The scratch lives
+ * in a fixed 15.7 MB device array of the library (held on every GPU that
+ * loads it), so meshes above 131072 tets are rejected with EMG_ERR_ARG.
+ * err_dev (n_err x T) and eta_dev (n_sol x T) are caller-owned device
+ * buffers laid out as in emg_estimate_error.  The first call on a device
+ * looks up the array's device address; make that call before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU (two
+ * contexts or threads at once) race.  Returns after the stream completes. */
+int emg_estimate_error_noalloc(emg_context *ctx, int fidx, int tidx, double *err_dev, double *eta_dev);
+
 /* refine_fixed_fraction / refine_fixed_number (src/em_fwd.cc:1182-1240):
  * ORs flags into flag[n] exactly as the reference. Host-side. */
 int emg_refine_fixed_fraction(int n, const double *err, double fraction, unsigned char *flag);
