@@ -37,6 +37,7 @@ void fail(int code, const char *fmt, ...) {
 
 static std::atomic<long> g_launches{0};
 long launch_count() { return g_launches.load(); }
+void add_launches(long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void launch_check(const char *file, int line) {
   g_launches.fetch_add(1, std::memory_order_relaxed);

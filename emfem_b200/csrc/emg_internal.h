@@ -54,6 +54,8 @@ struct KernelProfiler {
 };
 KernelProfiler &profiler();
 long launch_count();
+// a replayed CUDA graph runs the kernels captured into it: count them
+void add_launches(long n);
 
 // ---------------------------------------------------------------------------
 // device buffer (cudaMalloc-backed, move-only)

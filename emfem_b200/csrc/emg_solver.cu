@@ -462,6 +462,7 @@ void Ams<T>::apply(const T *b, T *x, cudaStream_t s) {
   auto it = graphs.exec.find(key);
   if (it != graphs.exec.end()) {
     EMG_CUDA(cudaGraphLaunch(it->second, s));
+    add_launches(graphs.kernels[key]);
     return;
   }
   if (graphs.seen[key]++ == 0) {
@@ -469,6 +470,7 @@ void Ams<T>::apply(const T *b, T *x, cudaStream_t s) {
     return;
   }
   cudaGraph_t g;
+  const long l0 = launch_count();
   EMG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   try {
     apply_eager(b, x, s);
@@ -483,6 +485,7 @@ void Ams<T>::apply(const T *b, T *x, cudaStream_t s) {
   cudaGraphDestroy(g);
   EMG_CUDA(e);
   graphs.exec[key] = ex;
+  graphs.kernels[key] = launch_count() - l0;  // counted at capture; the launch below runs them
   EMG_CUDA(cudaGraphLaunch(ex, s));
 }
 

@@ -17,15 +17,19 @@ namespace emg {
 struct GraphCache {
   std::map<std::pair<const void *, void *>, cudaGraphExec_t> exec;
   std::map<std::pair<const void *, void *>, int> seen;
+  std::map<std::pair<const void *, void *>, long> kernels;  // kernel nodes per graph
   GraphCache() = default;
   GraphCache(const GraphCache &) = delete;
   GraphCache &operator=(const GraphCache &) = delete;
-  GraphCache(GraphCache &&o) noexcept : exec(std::move(o.exec)), seen(std::move(o.seen)) { o.exec.clear(); }
+  GraphCache(GraphCache &&o) noexcept : exec(std::move(o.exec)), seen(std::move(o.seen)), kernels(std::move(o.kernels)) {
+    o.exec.clear();
+  }
   GraphCache &operator=(GraphCache &&o) noexcept {
     if (this != &o) {
       clear();
       exec = std::move(o.exec);
       seen = std::move(o.seen);
+      kernels = std::move(o.kernels);
       o.exec.clear();
     }
     return *this;
@@ -35,6 +39,7 @@ struct GraphCache {
     for (auto &kv : exec) cudaGraphExecDestroy(kv.second);
     exec.clear();
     seen.clear();
+    kernels.clear();
   }
 };
 

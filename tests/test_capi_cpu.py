@@ -1,0 +1,78 @@
+"""C ABI checks that need no GPU: every declared symbol is exported, options
+parsing (process_options, src/em_ctx.cc:100-175), host-side marking and
+argument/state errors."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+import emfem_b200 as E
+import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "emfem_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(emg_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = E.lib()
+    names = declared_symbols()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_options_parsing():
+    with E.EMContext(-1) as c:
+        c.process_options("""
+            -iprefix model -oprefix out   # file prefixes
+            -K_max_it 50 -e_rtol 1e-9 -dual_rtol 1e-7
+            -inner_pc_type ams -pc_threshold 1000 -refine_strategy fixed_number
+            -A_ksp_gmres_restart 20 -B_ksp_rtol 0.05 -B_ksp_max_it 40
+            -B_pc_hypre_ams_cycle_type 11 -A_ksp_monitor_true_residual
+            -emg_inner_precision fp32 -save_mesh 0
+        """)
+        assert c.get_option("K_max_it") == 50
+        assert c.get_option("e_rtol") == 1e-9
+        assert c.get_option("dual_rtol") == 1e-7
+        assert c.get_option("inner_pc_type") == 1
+        assert c.get_option("refine_strategy") == 0
+        assert c.get_option("A_ksp_gmres_restart") == 20
+        assert c.get_option("B_ksp_rtol") == 0.05
+        assert c.get_option("emg_inner_precision") == 1
+        assert c.get_option("save_mesh") == 0
+        for bad in ("-bogus 1", "-K_max_it abc", "-inner_pc_type lu", "-A_ksp_gmres_restart 99",
+                    "-B_pc_hypre_ams_cycle_type 5", "stray"):
+            with pytest.raises(E.EMGError) as ei:
+                c.process_options(bad)
+            assert ei.value.code == E.api.EMG_ERR_OPTION
+        # defaults of process_options are kept for untouched keys
+        assert c.get_option("refine_fraction") == 0.1
+
+
+def test_host_only_context_refuses_device_work():
+    with E.EMContext(-1) as c:
+        from emfem_b200 import meshgen as mg
+        prob = mg.mt_halfspace_block(800, freqs=(1.0,))
+        with pytest.raises(E.EMGError) as ei:
+            c.set_mesh(prob.mesh)
+        assert ei.value.code == E.api.EMG_ERR_STATE
+        with pytest.raises(E.EMGError):
+            c.create_linear_system(-3)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_refine_marking_matches_oracle(seed):
+    rng = np.random.default_rng(seed)
+    err = rng.lognormal(size=5000)
+    err[rng.integers(0, 5000, 50)] = err[0]            # ties
+    for frac in (0.05, 0.1, 0.3):
+        assert np.array_equal(E.refine_fixed_fraction(err, frac), O.refine_fixed_fraction(err, frac))
+        assert np.array_equal(E.refine_fixed_number(err, frac), O.refine_fixed_number(err, frac))
+    with pytest.raises(E.EMGError):
+        E.refine_fixed_number(err, 1.5)
