@@ -162,18 +162,25 @@ def columns(prob):
     return freqs, colf, modes
 
 
-def roofline_traffic(bin_name):
+def roofline_traffic(bin_name, algo_bytes_per_launch):
     """DRAM traffic per launch of the profiled kernel from the committed ncu
-    summary (profiles/<bin>_traffic.txt, line 'traffic_bytes_per_launch: X')."""
+    summary (profiles/<bin>_traffic.txt).  The capture is one launch of a
+    smaller case of the same kernel; its traffic / algorithmic-bytes ratio,
+    applied to this run's average algorithmic bytes per launch, gives the
+    traffic of a launch here (traffic grows with rows and nonzeros)."""
     path = os.path.join(ROOT, "profiles", bin_name + "_traffic.txt")
+    vals = {}
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":")[1])
-    except Exception:
-        pass
-    return None
+                if ":" in line and not line.startswith("#"):
+                    k, v = line.split(":", 1)
+                    vals[k.strip()] = float(v)
+    except OSError:
+        return None, None
+    if "traffic_over_algorithmic" in vals:
+        return vals["traffic_over_algorithmic"] * algo_bytes_per_launch, vals["traffic_over_algorithmic"]
+    return vals.get("traffic_bytes_per_launch"), None
 
 
 # ----------------------------------------------------------------------------
@@ -343,11 +350,14 @@ def ours(args):
     n_l, t_l, b_l = bins[dom]
     peak, peak_kind = peaks()
     achieved = (b_l / max(n_l, 1)) / ((t_l / max(n_l, 1)) * 1e-3) / 1e9 if n_l else 0.0
-    traffic = roofline_traffic(dom)
+    traffic, traffic_ratio = roofline_traffic(dom, b_l / max(n_l, 1))
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
             "algorithmic_bytes_per_launch": b_l / max(n_l, 1), "launches": n_l,
             "avg_launch_us": 1e3 * t_l / max(n_l, 1),
+            "traffic_source": ("ncu dram bytes / algorithmic bytes = %.3f on the committed capture "
+                               "(profiles/%s_traffic.txt), times this run's algorithmic bytes per launch"
+                               % (traffic_ratio, dom)) if traffic_ratio else None,
             "measured": "CUDA events around every launch of the kernel during one profiled step of this "
                         "workload (launch by launch) right after the timed region",
             "share_of_profiled_step": t_l / (prof_step_s * 1e3) if prof_step_s > 0 else None}
