@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--breakdown", action="store_true", help="print per-phase host timings to stderr")
+    ap.add_argument("--options", default="", help="extra solver options (process_options text)")
     return ap.parse_args()
 
 
@@ -275,6 +276,8 @@ def ours(args):
     K = colf.size
     bg = mg.background_model(prob.mesh, prob.model)
     ctx = E.EMContext(local)
+    if args.options:
+        ctx.process_options(args.options)
     ctx.set_mesh(prob.mesh)
     ctx.set_model(prob.model)
     ctx.set_frequencies(freqs)
@@ -339,11 +342,23 @@ def ours(args):
     torch.cuda.synchronize()
     prof_step_s = time.perf_counter() - tp0
     bins = {}
-    for b in ("spmm_edge_fp32", "spmm_edge_fp64", "spmm_nodal_fp32", "spmm_nodal_fp64"):
+    for b in ("spmm_edge_fp32", "spmm_edge_fp64", "spmm_nodal_fp32", "spmm_nodal_fp64", "vcycle_fused_fp32"):
         n, t, by = E.profile_get(b)
         bins[b] = (n, t, by)
     E.profile_enable(False)
     log("profiled step: %.1f s" % prof_step_s)
+    # solver phases with graphs and fused launches kept: events around the
+    # outer FGMRES, each inner FCG solve, each AMS application and each FP64
+    # operator apply
+    E.profile_enable(2)
+    step()
+    torch.cuda.synchronize()
+    phases = {}
+    for b in ("phase_fgmres", "phase_fcg", "phase_ams", "phase_opB"):
+        n, t, _ = E.profile_get(b)
+        phases[b[6:]] = {"count": n, "ms": round(t, 2)}
+    E.profile_enable(False)
+    log("phases: %s" % phases)
     conv = [(i.true_rel_res, i.outer_its) for i in infos_last]
     all_conv = all(i.reason == 0 and i.true_rel_res <= 1e-8 for i in infos_last)
     dom = max(bins, key=lambda b: bins[b][1])
@@ -436,12 +451,15 @@ def ours(args):
                        "nnz": int(ctx.make_sparsity_patterns()[0][-1]), "rhs_per_step": K, "freqs_hz":
                        [float(f) for f in freqs], "rtol": 1e-8, "inner": "FCG(FP64) + AMS(FP32)",
                        "warm_start": "none (zero guess)", "l2": "inputs larger than L2 (operator ~%.0f MB)" %
-                       (int(ctx.make_sparsity_patterns()[0][-1]) * 20 / 1e6), "parallelism": "replicas" if world > 1 else "1 GPU"},
+                       (int(ctx.make_sparsity_patterns()[0][-1]) * 20 / 1e6), "parallelism": "replicas" if world > 1 else "1 GPU",
+                       "options": args.options or None},
             "e2e": e2e, "plain_fp64": plain,
             "speedup_vs_plain_fp64": (value / world) / plain["value"] if plain else None,
             "converged": all_conv, "true_rel_res_max": max(c[0] for c in conv) if conv else None,
             "outer_its": [c[1] for c in conv],
             "roofline": roof, "profile_bins": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in bins.items()},
+            "phases_one_step": phases,
+            "host_breakdown_s_per_step": {k: round(v / args.steps, 3) for k, v in breakdown.items()},
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "wall_s": wall,
         }
         print(json.dumps(line), flush=True)

@@ -33,8 +33,13 @@ static inline double combined(const HCsr &A, long k, double w) {
   return A.vm.empty() ? A.vc[k] : A.vc[k] + w * A.vm[k];
 }
 
+// j couples with i in the AMG sense: j != i and, for a system, the same
+// function (fn empty: scalar problem)
+static inline bool same_fn(const std::vector<int> &fn, int i, int j) { return fn.empty() || fn[i] == fn[j]; }
+
 // j strongly influences i  <=>  -a_ij >= theta * max_{k != i} (-a_ik)
-static void strength(const HCsr &A, double w, double theta, std::vector<int> &srp, std::vector<int> &sci) {
+static void strength(const HCsr &A, double w, double theta, const std::vector<int> &fn, std::vector<int> &srp,
+                     std::vector<int> &sci) {
   const int n = A.n;
   std::vector<int> cnt(n + 1, 0);
   std::vector<double> mx(n, 0.0);
@@ -42,12 +47,12 @@ static void strength(const HCsr &A, double w, double theta, std::vector<int> &sr
   for (int i = 0; i < n; ++i) {
     double m = 0;
     for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
-      if (A.ci[k] != i) m = std::max(m, -combined(A, k, w));
+      if (A.ci[k] != i && same_fn(fn, i, A.ci[k])) m = std::max(m, -combined(A, k, w));
     mx[i] = m;
     int c = 0;
     if (m > 0)
       for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
-        if (A.ci[k] != i && -combined(A, k, w) >= theta * m) ++c;
+        if (A.ci[k] != i && same_fn(fn, i, A.ci[k]) && -combined(A, k, w) >= theta * m) ++c;
     cnt[i + 1] = c;
   }
   for (int i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
@@ -59,7 +64,7 @@ static void strength(const HCsr &A, double w, double theta, std::vector<int> &sr
     int p = srp[i];
     if (m > 0)
       for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
-        if (A.ci[k] != i && -combined(A, k, w) >= theta * m) sci[p++] = A.ci[k];
+        if (A.ci[k] != i && same_fn(fn, i, A.ci[k]) && -combined(A, k, w) >= theta * m) sci[p++] = A.ci[k];
   }
 }
 
@@ -131,8 +136,8 @@ static void pmis(int n, const std::vector<int> &srp, const std::vector<int> &sci
   }
 }
 
-static void direct_interp(const HCsr &A, double w, const std::vector<int> &srp, const std::vector<int> &sci,
-                          const std::vector<int> &cf, int pmax, HCsr &P) {
+static void direct_interp(const HCsr &A, double w, const std::vector<int> &fn, const std::vector<int> &srp,
+                          const std::vector<int> &sci, const std::vector<int> &cf, int pmax, HCsr &P) {
   const int n = A.n;
   std::vector<int> cidx(n, -1);
   int nc = 0;
@@ -157,6 +162,7 @@ static void direct_interp(const HCsr &A, double w, const std::vector<int> &srp, 
         int j = A.ci[k];
         double a = combined(A, k, w);
         if (j == i) { diag = a; continue; }
+        if (!same_fn(fn, i, j)) continue;
         if (a < 0) sn += a; else sp += a;
         if (cf[j] == 1 && strong[j]) { if (a < 0) cn += a; else cp += a; }
       }
@@ -287,14 +293,26 @@ HCsr spgemm(const HCsr &A, const HCsr &B) {
 void amg_build(const HCsr &A0, double w_ref, const AmgParams &prm, HostAmg &out) {
   out.lv.clear();
   HCsr A = A0;
+  std::vector<int> fn;
+  if (prm.num_functions > 1) {
+    fn.resize(A.n);
+    for (int i = 0; i < A.n; ++i) fn[i] = i % prm.num_functions;
+  }
   for (int l = 0;; ++l) {
     if (A.n <= prm.max_coarse || l + 1 >= prm.max_levels) break;
     std::vector<int> srp, sci, cf;
-    strength(A, w_ref, prm.theta, srp, sci);
+    strength(A, w_ref, prm.theta, fn, srp, sci);
     pmis(A.n, srp, sci, prm.seed + (uint64_t)l, cf);
     HCsr P;
-    direct_interp(A, w_ref, srp, sci, cf, prm.pmax, P);
+    direct_interp(A, w_ref, fn, srp, sci, cf, prm.pmax, P);
     if (P.m == 0 || P.m > 0.95 * A.n) break;
+    if (!fn.empty()) {  // a coarse point keeps its function
+      std::vector<int> fc;
+      fc.reserve(P.m);
+      for (int i = 0; i < A.n; ++i)
+        if (cf[i] == 1) fc.push_back(fn[i]);
+      fn.swap(fc);
+    }
     HCsr R = transpose(P);
     HCsr AP = spgemm(A, P);
     HCsr RAP;

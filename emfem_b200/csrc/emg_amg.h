@@ -14,6 +14,10 @@ struct AmgParams {
   int max_coarse = 200;
   int max_levels = 25;
   uint64_t seed = 12345;
+  // systems AMG, unknown approach: row i carries function i % num_functions
+  // on the finest level; strength and interpolation only couple rows of the
+  // same function (the coarse operators still couple them through R A P)
+  int num_functions = 1;
 };
 
 struct HostLevel {

@@ -462,6 +462,118 @@ void assemble_nodal(Context &c, HCsr out[4]) {
   }
 }
 
+// The vector nodal space of AMS (hypre's Pi space, cycle character '2'):
+// Pi = [Pi_x Pi_y Pi_z] interpolates a vertex vector field (3 values per
+// vertex) onto the edges, and Pi^T K Pi couples the three components.  The
+// nine 4x4 element blocks Q_d1^T K Q_d2 are summed into nine vertex-pattern
+// arrays per value part; the host interleaves them as row 3 v + d1, column
+// 3 u + d2.
+struct PiOut {
+  double *v[18];  // (d1 * 3 + d2) * 2 + part
+};
+
+__global__ void __launch_bounds__(128) assemble_pivec_kernel(ElemIn in, int nt, const int *__restrict__ vslot,
+                                                              PiOut out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  double c[36], m[36];
+  TetGeom g;
+  element_matrices(in, t, c, m, g);
+  int vs[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) vs[k] = __ldg(vslot + 16 * (long)t + k);
+  // w[k][d]: Pi_d weight of edge k at both of its endpoints
+  double w[6][3];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const int a = kEdgeP(k), b = kEdgeQ(k);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) w[k][d] = 0.5 * (g.x[b][d] - g.x[a][d]);
+  }
+#pragma unroll
+  for (int part = 0; part < 2; ++part) {
+    const double *K = part == 0 ? c : m;
+#pragma unroll 1
+    for (int d2 = 0; d2 < 3; ++d2) {
+      // KQ = K Q_d2 (6 x 4)
+      double KQ[6][4];
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) KQ[i][q] = 0.0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const int a = kEdgeP(j), b = kEdgeQ(j);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          const double v = K[i * 6 + j] * w[j][d2];
+          KQ[i][a] += v;
+          KQ[i][b] += v;
+        }
+      }
+#pragma unroll 1
+      for (int d1 = 0; d1 < 3; ++d1) {
+        double B[4][4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) B[p][q] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          const int a = kEdgeP(i), b = kEdgeQ(i);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const double v = w[i][d1] * KQ[i][q];
+            B[a][q] += v;
+            B[b][q] += v;
+          }
+        }
+        double *o = out.v[(d1 * 3 + d2) * 2 + part];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) atomicAdd(o + vs[p * 4 + q], B[p][q]);
+      }
+    }
+  }
+}
+
+void assemble_pi_vector(Context &c, HCsr &out, bool coupled) {
+  const long vnnz = c.h_vrp[c.nv];
+  DBuf<double> buf((size_t)vnnz * 18);
+  buf.zero(c.stream);
+  PiOut o;
+  for (int k = 0; k < 18; ++k) o.v[k] = buf.p + (size_t)k * vnnz;
+  assemble_pivec_kernel<<<(unsigned)((c.nt + 127) / 128), 128, 0, c.stream>>>(elem_in(c), c.nt, c.vslot.p, o);
+  EMG_LAUNCH_CHECK();
+  std::vector<double> h((size_t)vnnz * 18);
+  buf.download(h.data(), h.size(), c.stream);
+  EMG_CUDA(cudaStreamSynchronize(c.stream));
+  const int nv = c.nv;
+  out.n = out.m = 3 * nv;
+  out.rp.assign(3 * (size_t)nv + 1, 0);
+  const int nb = coupled ? 3 : 1;  // column blocks per row: all three components, or its own
+  for (int v = 0; v < nv; ++v)
+    for (int d = 0; d < 3; ++d) out.rp[3 * v + d + 1] = nb * (c.h_vrp[v + 1] - c.h_vrp[v]);
+  for (int i = 0; i < 3 * nv; ++i) out.rp[i + 1] += out.rp[i];
+  out.ci.resize(out.rp[3 * nv]);
+  out.vc.resize(out.rp[3 * nv]);
+  out.vm.resize(out.rp[3 * nv]);
+#pragma omp parallel for schedule(static)
+  for (int v = 0; v < nv; ++v)
+    for (int d1 = 0; d1 < 3; ++d1) {
+      long p = out.rp[3 * v + d1];
+      for (int k = c.h_vrp[v]; k < c.h_vrp[v + 1]; ++k)
+        for (int d2 = 0; d2 < 3; ++d2) {
+          if (!coupled && d2 != d1) continue;
+          out.ci[p] = 3 * c.h_vci[k] + d2;
+          out.vc[p] = h[(size_t)((d1 * 3 + d2) * 2) * vnnz + k];
+          out.vm[p] = h[(size_t)((d1 * 3 + d2) * 2 + 1) * vnnz + k];
+          ++p;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // G^T B as a vertex x edge operator.  The gradient-space residual of AMS,
 // G^T (b - B x), is formed as G^T b - (G^T B) x: G^T C vanishes exactly on

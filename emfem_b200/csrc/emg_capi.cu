@@ -197,9 +197,15 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "B_ksp_fcg_mmax") o.fcg_mmax = geti(k, v);
     else if (key == "B_pc_hypre_ams_cycle_type") {
       int ct = geti(k, v);
-      if (ct == 13) o.ams_cycle = "034515430";
+      // hypre's multiplicative AMS cycles: 0 edge smoothing, 1 gradient
+      // space, 2 vector Pi space, 3/4/5 its x/y/z components
+      if (ct == 1) o.ams_cycle = "01210";
+      else if (ct == 3) o.ams_cycle = "02120";
+      else if (ct == 5) o.ams_cycle = "0102010";
+      else if (ct == 7) o.ams_cycle = "0201020";
       else if (ct == 11) o.ams_cycle = "013454310";
-      else fail(EMG_ERR_OPTION, "AMS cycle type %d is not implemented (11 and 13 are)", ct);
+      else if (ct == 13) o.ams_cycle = "034515430";
+      else fail(EMG_ERR_OPTION, "AMS cycle type %d is not implemented (1, 3, 5, 7, 11 and 13 are)", ct);
     } else if (key == "B_pc_hypre_ams_relax_times") o.ams_relax_times = geti(k, v);
     else if (key == "B_pc_hypre_ams_relax_weight") o.ams_relax_weight = getr(k, v);
     else if (key == "B_pc_hypre_ams_amg_alpha_theta" || key == "B_pc_hypre_ams_amg_beta_theta") o.amg_theta = getr(k, v);
@@ -212,6 +218,10 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_smoother") o.smoother_cheb = elist(k, v, {"l1jacobi", "chebyshev"});
     else if (key == "emg_fp32_cycle") o.fp32_cycle = v;
     else if (key == "emg_graphs") o.graphs = v.empty() ? 1 : getb(v);
+    else if (key == "emg_fused_vcycle") o.ams_fused = v.empty() ? 1 : getb(v);
+    else if (key == "emg_fused_blocks_per_sm") o.fused_bps = geti(k, v);
+    else if (key == "emg_fused_rows") o.fused_rows = geti(k, v);
+    else if (key == "emg_pi_coupled") o.pi_coupled = v.empty() ? 1 : getb(v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
     else if (key.rfind("A_", 0) == 0 || key.rfind("B_", 0) == 0) ignored.push_back(k);
     else fail(EMG_ERR_OPTION, "unknown option %s", k.c_str());
@@ -334,65 +344,115 @@ struct PlaneWave1D {
 
 // calculate_boundary_values (src/em_fwd.cc:402-486): Dirichlet value of every
 // boundary edge (first encounter in ascending tet order wins)
-static void boundary_values(Context &c, double freq, int mode, std::vector<std::complex<double>> &bv,
-                            const std::vector<unsigned char> &bdr_cell) {
-  typedef std::complex<double> zc;
+// Geometry of the MT boundary values (assemble_rhs_mt, src/em_fwd.cc:488-580)
+// that does not depend on frequency or polarisation: per boundary edge its
+// midpoint depth, the blend weights of the four corner soundings and the
+// tangential components.  Each edge is evaluated in the lowest-numbered
+// boundary tet that holds it, as the reference's tet loop does.
+struct MtBoundary {
+  std::vector<int> edge, zslot;
+  std::vector<double> co, ed, den;  // 4, 2 and 1 per edge
+  std::vector<double> zs;           // distinct midpoint depths
+};
+
+static void mt_boundary_geometry(Context &c, const std::vector<unsigned char> &bdr_cell, MtBoundary &g) {
   need(!c.bg_nlay.empty(), EMG_ERR_STATE, "MT right-hand side needs emg_set_background first");
-  PlaneWave1D pw[4];
-  for (int q = 0; q < 4; ++q) pw[q].init(&c.bg_ztop[q * c.bg_maxl], &c.bg_lsig[q * c.bg_maxl], c.bg_nlay[q], freq);
   const double *tc = c.bg_corners.data();
   auto T = [&](int q, int d) { return tc[3 * q + d]; };
-  bv.assign(c.ne, zc(0));
   std::vector<char> have(c.ne, 0);
+  std::vector<int> tet, loc;
+  g.edge.clear();
   for (int t = 0; t < c.nt; ++t) {
     if (!bdr_cell[t]) continue;
-    HostTet h;
-    host_tet(c, t, h);
     for (int i = 0; i < 6; ++i) {
       int e = c.h_t2e[6 * (size_t)t + i];
       if (!c.h_ebdr[e] || have[e]) continue;
-      const double *p0 = &c.h_pts[3 * (size_t)c.h_edges[2 * (size_t)e]];
-      const double *p1 = &c.h_pts[3 * (size_t)c.h_edges[2 * (size_t)e + 1]];
-      double ec[3], ed[3];
-      for (int d = 0; d < 3; ++d) {
-        ec[d] = (p0[d] + p1[d]) / 2.0;
-        ed[d] = p1[d] - p0[d];
-      }
-      double co[4];
-      if (std::fabs(ec[0] - T(0, 0)) < EPS) {
-        double w = (1.0 - std::cos(PI * (ec[1] - T(0, 1)) / (T(2, 1) - T(0, 1)))) / 2.0;
-        co[0] = 1.0 - w; co[1] = 0.0; co[2] = 0.0; co[3] = w;
-      } else if (std::fabs(ec[1] - T(0, 1)) < EPS) {
-        double w = (1.0 - std::cos(PI * (ec[0] - T(0, 0)) / (T(2, 0) - T(0, 0)))) / 2.0;
-        co[0] = 1.0 - w; co[1] = w; co[2] = 0.0; co[3] = 0.0;
-      } else if (std::fabs(ec[0] - T(2, 0)) < EPS) {
-        double w = (1.0 - std::cos(PI * (ec[1] - T(0, 1)) / (T(2, 1) - T(0, 1)))) / 2.0;
-        co[0] = 0.0; co[1] = 1.0 - w; co[2] = w; co[3] = 0.0;
-      } else if (std::fabs(ec[1] - T(2, 1)) < EPS) {
-        double w = (1.0 - std::cos(PI * (ec[0] - T(0, 0)) / (T(2, 0) - T(0, 0)))) / 2.0;
-        co[0] = 0.0; co[1] = 0.0; co[2] = w; co[3] = 1.0 - w;
-      } else {
-        double area = (T(2, 0) - T(0, 0)) * (T(2, 1) - T(0, 1));
-        co[0] = ((T(2, 0) - ec[0]) * (T(2, 1) - ec[1])) / area;
-        co[1] = ((ec[0] - T(3, 0)) * (T(3, 1) - ec[1])) / area;
-        co[2] = ((ec[0] - T(0, 0)) * (ec[1] - T(0, 1))) / area;
-        co[3] = ((T(1, 0) - ec[0]) * (ec[1] - T(1, 1))) / area;
-      }
-      zc ep[3] = {0.0, 0.0, 0.0};
-      for (int q = 0; q < 4; ++q) {
-        zc eh[4];
-        pw[q].field(ec[2], eh);
-        if (mode == EMG_SOL_MT_XY) ep[0] += co[q] * std::conj(eh[0]);
-        else if (mode == EMG_SOL_MT_YX) ep[1] += co[q] * std::conj(eh[2]);
-      }
-      double phi[3];
-      int ge;
-      host_phi(c, h, t, i, ec, phi, &ge);
-      zc num = ed[0] * ep[0] + ed[1] * ep[1] + ed[2] * ep[2];
-      zc dof = num / (ed[0] * phi[0] + ed[1] * phi[1] + ed[2] * phi[2]);
       have[e] = 1;
-      bv[e] = std::abs(dof) > 1E-13 ? dof : zc(0.0);
+      g.edge.push_back(e);
+      tet.push_back(t);
+      loc.push_back(i);
     }
+  }
+  const int nb = (int)g.edge.size();
+  std::vector<double> z(nb);
+  g.co.assign(4 * (size_t)nb, 0.0);
+  g.ed.assign(2 * (size_t)nb, 0.0);
+  g.den.assign(nb, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; ++b) {
+    const int e = g.edge[b], t = tet[b], i = loc[b];
+    HostTet h;
+    host_tet(c, t, h);
+    const double *p0 = &c.h_pts[3 * (size_t)c.h_edges[2 * (size_t)e]];
+    const double *p1 = &c.h_pts[3 * (size_t)c.h_edges[2 * (size_t)e + 1]];
+    double ec[3], ed[3];
+    for (int d = 0; d < 3; ++d) {
+      ec[d] = (p0[d] + p1[d]) / 2.0;
+      ed[d] = p1[d] - p0[d];
+    }
+    double *co = &g.co[4 * (size_t)b];
+    if (std::fabs(ec[0] - T(0, 0)) < EPS) {
+      double w = (1.0 - std::cos(PI * (ec[1] - T(0, 1)) / (T(2, 1) - T(0, 1)))) / 2.0;
+      co[0] = 1.0 - w; co[1] = 0.0; co[2] = 0.0; co[3] = w;
+    } else if (std::fabs(ec[1] - T(0, 1)) < EPS) {
+      double w = (1.0 - std::cos(PI * (ec[0] - T(0, 0)) / (T(2, 0) - T(0, 0)))) / 2.0;
+      co[0] = 1.0 - w; co[1] = w; co[2] = 0.0; co[3] = 0.0;
+    } else if (std::fabs(ec[0] - T(2, 0)) < EPS) {
+      double w = (1.0 - std::cos(PI * (ec[1] - T(0, 1)) / (T(2, 1) - T(0, 1)))) / 2.0;
+      co[0] = 0.0; co[1] = 1.0 - w; co[2] = w; co[3] = 0.0;
+    } else if (std::fabs(ec[1] - T(2, 1)) < EPS) {
+      double w = (1.0 - std::cos(PI * (ec[0] - T(0, 0)) / (T(2, 0) - T(0, 0)))) / 2.0;
+      co[0] = 0.0; co[1] = 0.0; co[2] = w; co[3] = 1.0 - w;
+    } else {
+      double area = (T(2, 0) - T(0, 0)) * (T(2, 1) - T(0, 1));
+      co[0] = ((T(2, 0) - ec[0]) * (T(2, 1) - ec[1])) / area;
+      co[1] = ((ec[0] - T(3, 0)) * (T(3, 1) - ec[1])) / area;
+      co[2] = ((ec[0] - T(0, 0)) * (ec[1] - T(0, 1))) / area;
+      co[3] = ((T(1, 0) - ec[0]) * (ec[1] - T(1, 1))) / area;
+    }
+    double phi[3];
+    int ge;
+    host_phi(c, h, t, i, ec, phi, &ge);
+    g.ed[2 * (size_t)b] = ed[0];
+    g.ed[2 * (size_t)b + 1] = ed[1];
+    g.den[b] = ed[0] * phi[0] + ed[1] * phi[1] + ed[2] * phi[2];
+    z[b] = ec[2];
+  }
+  g.zs = z;
+  std::sort(g.zs.begin(), g.zs.end());
+  g.zs.erase(std::unique(g.zs.begin(), g.zs.end()), g.zs.end());
+  g.zslot.resize(nb);
+  for (int b = 0; b < nb; ++b) g.zslot[b] = (int)(std::lower_bound(g.zs.begin(), g.zs.end(), z[b]) - g.zs.begin());
+}
+
+// boundary DOF values of one (frequency, polarisation): the 1-D plane-wave
+// field of the four corner soundings at each distinct depth, blended per edge
+static void boundary_values(Context &c, const MtBoundary &g, double freq, int mode, std::vector<std::complex<double>> &bv) {
+  typedef std::complex<double> zc;
+  PlaneWave1D pw[4];
+  for (int q = 0; q < 4; ++q) pw[q].init(&c.bg_ztop[q * c.bg_maxl], &c.bg_lsig[q * c.bg_maxl], c.bg_nlay[q], freq);
+  const int nz = (int)g.zs.size(), nb = (int)g.edge.size();
+  // polarisation XY drives E_x (field component 0), YX drives E_y (component 2)
+  const int comp = mode == EMG_SOL_MT_XY ? 0 : 2;
+  std::vector<zc> f(4 * (size_t)nz);
+#pragma omp parallel for schedule(static)
+  for (int iz = 0; iz < nz; ++iz)
+    for (int q = 0; q < 4; ++q) {
+      zc eh[4];
+      pw[q].field(g.zs[iz], eh);
+      f[4 * (size_t)iz + q] = std::conj(eh[comp]);
+    }
+  bv.assign(c.ne, zc(0));
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; ++b) {
+    const double *co = &g.co[4 * (size_t)b];
+    const zc *fz = &f[4 * (size_t)g.zslot[b]];
+    zc ep[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < 4; ++q) ep[comp == 0 ? 0 : 1] += co[q] * fz[q];
+    const double ed0 = g.ed[2 * (size_t)b], ed1 = g.ed[2 * (size_t)b + 1];
+    zc num = ed0 * ep[0] + ed1 * ep[1];
+    zc dof = num / g.den[b];
+    bv[g.edge[b]] = std::abs(dof) > 1E-13 ? dof : zc(0.0);
   }
 }
 
@@ -508,6 +568,11 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "B_ksp_max_it") *value = o.inner_max_it;
   else if (k == "B_ksp_fcg_mmax") *value = o.fcg_mmax;
   else if (k == "emg_inner_precision") *value = o.inner_fp32;
+  else if (k == "emg_graphs") *value = o.graphs;
+  else if (k == "emg_fused_vcycle") *value = o.ams_fused;
+  else if (k == "emg_fused_blocks_per_sm") *value = o.fused_bps;
+  else if (k == "emg_fused_rows") *value = o.fused_rows;
+  else if (k == "emg_pi_coupled") *value = o.pi_coupled;
   else fail(EMG_ERR_OPTION, "unknown option %s", key);
   EMG_API_END
 }
@@ -752,6 +817,7 @@ int emg_pc_apply_b(emg_context *c, const double *b, double *x) {
   std::vector<double> xo((size_t)n * 2);
   w.vec_b.download(xo.data(), xo.size(), c->stream);
   EMG_CUDA(cudaStreamSynchronize(c->stream));
+  w.pams64.check_fused(c->stream);
   for (int i = 0; i < n; ++i) {
     x[i] = xo[2 * (size_t)i];
     x[n + i] = xo[2 * (size_t)i + 1];
@@ -790,6 +856,8 @@ int emg_solve_linear_system(emg_context *c, int target, const double *s_re, cons
     w.fcg64.solve(w.pams64, v, z, c->opt.inner_rtol, c->opt.inner_max_it, c->stream);
   };
   w.gm.solve(*c, w.vec_a.p, x.p, false, rtol, max_it, true, pc, st);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  w.pams64.check_fused(c->stream);
   fill_info(info, st, w.fcg64.total_its, 0);
   c->kernel_ms["solve"] = st.seconds * 1e3;
   if (!st.converged[0]) fail(EMG_DIVERGED_ITS, "FGMRES reached %d iterations at relative residual %.3e", max_it,
@@ -846,9 +914,12 @@ static void rhs_mt_block(Context &c, int k, const double *freqs, const int *mode
   c.bdr_cell.download(bdr.data(), c.nt, c.stream);
   EMG_CUDA(cudaStreamSynchronize(c.stream));
   std::vector<double> bv((size_t)c.ne * k * 2, 0.0), om(k);
+  MtBoundary g;
+  mt_boundary_geometry(c, bdr, g);
   for (int j = 0; j < k; ++j) {
     std::vector<std::complex<double>> v;
-    boundary_values(c, freqs[j], modes[j], v, bdr);
+    boundary_values(c, g, freqs[j], modes[j], v);
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < c.ne; ++e) {
       bv[2 * ((size_t)e * k + j)] = v[e].real();
       bv[2 * ((size_t)e * k + j) + 1] = v[e].imag();
@@ -1135,24 +1206,43 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     a.relax_w = 1.0;
     a.mode = SPMM_AX;
     KernelProfiler &pf = profiler();
-    cudaEvent_t ev = nullptr;
+    cudaEvent_t ev = nullptr, ph = nullptr;
     if (pf.enabled)
       pf.begin("spmm_edge_fp64", c.stream, spmm_algo_bytes(n, c.nnz, K2, 8, true, SPMM_AX), &ev);
+    if (pf.phases) pf.begin("phase_opB", c.stream, 0, &ph);
     spmm_nnz<double>(K2, a, c.nnz, c.stream);
     if (pf.enabled) pf.end("spmm_edge_fp64", c.stream, ev);
+    if (pf.phases) pf.end("phase_opB", c.stream, ph);
   };
   auto pc32 = [&](const double *r_, double *z_) {
+    KernelProfiler &pf = profiler();
+    cudaEvent_t ph = nullptr;
+    if (pf.phases) pf.begin("phase_ams", c.stream, 0, &ph);
     cvt_d2f((long)n * K2, r_, w.f_in.p, c.stream);
     w.bams32.apply(w.f_in.p, w.f_out.p, c.stream);
     add_gradient_f2d(n, K2, c.edges.p, w.f_out.p, w.bams32.gphi(), z_, c.stream);
+    if (pf.phases) pf.end("phase_ams", c.stream, ph);
   };
   auto pc = [&](const double *v, double *z) {
+    KernelProfiler &pf = profiler();
+    cudaEvent_t ph = nullptr;
+    if (pf.phases) pf.begin("phase_fcg", c.stream, 0, &ph);
     if (fp32) w.fcg64.solve_with(n, K2, pc32, opB64, v, z, c.opt.inner_rtol, c.opt.inner_max_it, c.stream);
     else w.fcg64.solve(w.bams64, v, z, c.opt.inner_rtol, c.opt.inner_max_it, c.stream);
+    if (pf.phases) pf.end("phase_fcg", c.stream, ph);
   };
   SolveStats st;
-  w.gm.solve(c, w.vec_a.p, x_dev, o.use_guess != 0, o.rtol > 0 ? o.rtol : c.opt.e_rtol,
-             o.max_it > 0 ? o.max_it : c.opt.K_max_it, false, pc, st);
+  {
+    KernelProfiler &pf = profiler();
+    cudaEvent_t ph = nullptr;
+    if (pf.phases) pf.begin("phase_fgmres", c.stream, 0, &ph);
+    w.gm.solve(c, w.vec_a.p, x_dev, o.use_guess != 0, o.rtol > 0 ? o.rtol : c.opt.e_rtol,
+               o.max_it > 0 ? o.max_it : c.opt.K_max_it, false, pc, st);
+    if (pf.phases) pf.end("phase_fgmres", c.stream, ph);
+  }
+  EMG_CUDA(cudaStreamSynchronize(c.stream));
+  if (fp32) w.bams32.check_fused(c.stream);
+  else w.bams64.check_fused(c.stream);
   long inner = w.fcg64.total_its;
   if (infos)
     for (int j = 0; j < k; ++j) fill_info(&infos[j], st, inner, j);
@@ -1222,7 +1312,8 @@ int emg_profile_enable(int on) {
   EMG_API_BEGIN
   KernelProfiler &p = profiler();
   p.reset();
-  p.enabled = on != 0;
+  p.enabled = on == 1;
+  p.phases = on == 2;
   EMG_API_END
 }
 

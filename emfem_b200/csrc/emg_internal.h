@@ -39,7 +39,8 @@ void launch_check(const char *file, int line);
 // start/stop event pair on the launching stream plus the launch's
 // algorithmic bytes.  Disabled unless enabled through the C ABI.
 struct KernelProfiler {
-  bool enabled = false;
+  bool enabled = false;  // every kernel launch timed (AMS runs eagerly)
+  bool phases = false;   // solver phases timed (graphs and fused launches kept)
   struct Rec {
     cudaEvent_t a, b;
     double bytes;
@@ -157,6 +158,10 @@ struct Options {
   // emg_*
   int inner_fp32 = 0;
   int graphs = 1;
+  int ams_fused = 0;          // small nodal levels as one cooperative launch per V-cycle
+  int fused_bps = 0;          // its resident blocks per SM cap (0: occupancy limit)
+  int fused_rows = 1 << 30;   // levels below this many rows run fused
+  int pi_coupled = 1;         // vector Pi space with (1) or without (0) its x/y/z couplings
   int verbose = 0;
 };
 
@@ -230,6 +235,9 @@ void canonicalize(Context &c);            // device: sorted tets + canonical edg
 void build_slot_maps(Context &c);         // device: tet -> CSR slots
 void assemble_edge(Context &c);           // device: C, Ms, bdr cells
 void assemble_nodal(Context &c, HCsr out[4]);  // device + download (G, Pi_x, Pi_y, Pi_z)
+// Pi^T K Pi, 3 nv rows, row 3 v + d; coupled = false keeps only the x/y/z
+// diagonal blocks (the three component spaces side by side, corrected at once)
+void assemble_pi_vector(Context &c, HCsr &out, bool coupled);
 void build_gtb_pattern(Context &c);       // host pattern + device slot map of G^T B
 void assemble_gtb(Context &c, DBuf<double> &gc, DBuf<double> &gm);  // G^T C (boundary part), G^T Ms
 void create_pc(Context &c, bool per_frequency_hierarchy, const std::vector<double> &omegas);

@@ -379,8 +379,22 @@ __global__ void ams_restrict_kernel(int nv, int K, int sp, const int *__restrict
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= (long)nv * K) return;
   int v = (int)(i / K), c = (int)(i % K);
-  T acc = 0;
   const int kb = __ldg(inc_rp + v), ke = __ldg(inc_rp + v + 1);
+  if (sp == 4) {  // vector space: rows 3 v + d
+    T a0 = 0, a1 = 0, a2 = 0;
+    for (int k = kb; k < ke; ++k) {
+      int e = __ldg(inc + k) >> 1;
+      T r = T(0.5) * __ldg(r_edge + (long)e * K + c);
+      a0 += __ldg(tangent + 3 * (long)e) * r;
+      a1 += __ldg(tangent + 3 * (long)e + 1) * r;
+      a2 += __ldg(tangent + 3 * (long)e + 2) * r;
+    }
+    r_vert[(3 * (long)v) * K + c] = a0;
+    r_vert[(3 * (long)v + 1) * K + c] = a1;
+    r_vert[(3 * (long)v + 2) * K + c] = a2;
+    return;
+  }
+  T acc = 0;
   for (int k = kb; k < ke; ++k) {
     int code = __ldg(inc + k);
     int e = code >> 1;
@@ -408,10 +422,19 @@ __global__ void ams_prolong_kernel(int ne, int K, int sp, const int *__restrict_
   if (i >= (long)ne * K) return;
   int e = (int)(i / K), c = (int)(i % K);
   int v0 = __ldg(edges + 2 * (long)e), v1 = __ldg(edges + 2 * (long)e + 1);
-  T a = __ldg(ev + (long)v0 * K + c), b = __ldg(ev + (long)v1 * K + c);
   T val;
-  if (sp == 0) val = b - a;
-  else val = T(0.5) * __ldg(tangent + 3 * (long)e + (sp - 1)) * (a + b);
+  if (sp == 4) {  // vector space: rows 3 v + d
+    val = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      val += __ldg(tangent + 3 * (long)e + d) *
+             (__ldg(ev + (3 * (long)v0 + d) * K + c) + __ldg(ev + (3 * (long)v1 + d) * K + c));
+    val *= T(0.5);
+  } else {
+    T a = __ldg(ev + (long)v0 * K + c), b = __ldg(ev + (long)v1 * K + c);
+    if (sp == 0) val = b - a;
+    else val = T(0.5) * __ldg(tangent + 3 * (long)e + (sp - 1)) * (a + b);
+  }
   x[i] += val;
 }
 

@@ -82,6 +82,22 @@ struct SpmmArgs {
   double c1, c2;           // Chebyshev coefficients (inv_theta in c1 for CHEB1)
 };
 
+// One step of a fused nodal V-cycle (vcycle_fused_kernel): the operations a
+// V-cycle launches one by one, recorded with their arguments and replayed in
+// order inside one cooperative launch with a grid barrier between steps.
+enum FusedKind : int {
+  FOP_SPMM = 0,    // SpMM in any mode (a: all fields)
+  FOP_JAC0 = 1,    // y = w b / d                 (a: n, b, l1c, l1m, omega, relax_w, y)
+  FOP_JAC0_2 = 2,  // y = d = w b / d             (a: n, b, l1c, l1m, omega, relax_w, y, d)
+  FOP_COARSE = 3,  // x = inv(slot(c)) b, dense   (a: n = nc, b, y = x, vc = FP64 inverses, ci = column slots)
+};
+
+struct FusedOp {
+  int kind;
+  long nnz;        // nonzeros of an SpMM (algorithmic bytes)
+  SpmmArgs a;
+};
+
 template <typename T, int K, int V, int NL>
 __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
   constexpr int CL = K / V;
@@ -108,24 +124,35 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
   const bool valid = row < a.n;
   if (valid) {
     const int kb = __ldg(a.rp + row), ke = __ldg(a.rp + row + 1);
-    if (two) {
-      for (int k = kb + sl; k < ke; k += NL) {
-        const int j = __ldg(a.ci + k);
-        const T c = __ldg(vc + k), m = __ldg(vm + k);
-        T xv[V];
-        ldv<T, V>(x + (long)j * K + cb * V, xv);
+    // U nonzeros per lane per round: all index/value loads of the round are
+    // issued before the dependent x gathers, so U gathers are in flight at
+    // once (rows are short, ~16 nonzeros, and split NL ways)
+    constexpr int U = 4;
+    for (int k0 = kb + sl; k0 < ke; k0 += NL * U) {
+      int j[U];
+      T c[U], m[U];
+      bool ok[U];
 #pragma unroll
-        for (int i = 0; i < V; ++i) acc[i] = fma(c + w[i] * m, xv[i], acc[i]);
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * NL;
+        ok[u] = k < ke;
+        j[u] = ok[u] ? __ldg(a.ci + k) : 0;
+        c[u] = ok[u] ? __ldg(vc + k) : T(0);
+        m[u] = (ok[u] && two) ? __ldg(vm + k) : T(0);
       }
-    } else {
-      for (int k = kb + sl; k < ke; k += NL) {
-        const int j = __ldg(a.ci + k);
-        const T c = __ldg(vc + k);
-        T xv[V];
-        ldv<T, V>(x + (long)j * K + cb * V, xv);
+      T xv[U][V];
 #pragma unroll
-        for (int i = 0; i < V; ++i) acc[i] = fma(c, xv[i], acc[i]);
+      for (int u = 0; u < U; ++u) {
+        if (ok[u]) ldv<T, V>(x + (long)j[u] * K + cb * V, xv[u]);
+        else {
+#pragma unroll
+          for (int i = 0; i < V; ++i) xv[u][i] = T(0);
+        }
       }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int i = 0; i < V; ++i) acc[i] = fma(two ? c[u] + w[i] * m[u] : c[u], xv[u][i], acc[i]);
     }
   }
 #pragma unroll

@@ -64,6 +64,7 @@ void fill_zero(long count, T *a, cudaStream_t s);
 // AMS transfers between edges and vertices for K columns.
 //   sp == 0: gradient G (row e: -1 at edges[e][0], +1 at edges[e][1])
 //   sp == 1..3: Pi_d, d = sp-1 (row e: 0.5 t_e[d] at both endpoints)
+//   sp == 4: Pi = [Pi_x Pi_y Pi_z], vertex vectors stored as rows 3 v + d
 template <typename T>
 void ams_restrict(int nv, int K, int sp, const int *inc_rp, const int *inc, const T *tangent, const T *r_edge,
                   T *r_vert, cudaStream_t s);
@@ -73,6 +74,14 @@ void ams_prolong_add(int ne, int K, int sp, const int *edges, const T *tangent, 
 // x[i,c] = sum_j inv[slot(c)][i][j] b[j,c]  (FP64 generalized inverse of the coarsest operator)
 template <typename T>
 void coarse_apply(int nc, int K, const double *inv, const int *col_slot, const T *b, T *x, cudaStream_t s);
+
+// One nodal V-cycle as a single cooperative launch (emg_fused.cu): runs the
+// recorded steps in order with a grid barrier between them.  bar: two words,
+// zero before the first launch (every launch leaves them consistent); err:
+// set nonzero when a barrier wait gave up, which ends the launch early.
+// max_bps caps the resident blocks per SM (0: the occupancy limit).
+template <typename T>
+void vcycle_fused(int K, const FusedOp *ops, int nops, unsigned *bar, int *err, int max_bps, cudaStream_t s);
 
 // ---- complex (FP64) kernels of the outer FGMRES ------------------------------
 // y = b - A(w_c) x  or  y = A(w_c) x, complex n x K; conj_out conjugates the

@@ -111,6 +111,10 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   ams.cheb = c.opt.smoother_cheb;
   ams.two = !per_frequency;
   ams.use_graphs = c.opt.graphs != 0;
+  ams.fused = c.opt.ams_fused != 0;
+  ams.fused_bps = c.opt.fused_bps;
+  ams.fused_rows = c.opt.fused_rows;
+  ams.fused_epoch = -1;
   // FP32 applications close with the gradient correction and hand it back
   // as a potential: after it, no FP32 product touches the (air) gradient
   // component, which can exceed the rest of the iterate by 1e10 at low
@@ -175,49 +179,56 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
     EMG_LAUNCH_CHECK();
     EMG_CUDA(cudaStreamSynchronize(s));
   }
-  // nodal subspace operators and their hierarchies
-  HCsr nod[4];
-  assemble_nodal(c, nod);
+  // nodal subspace operators (only those the cycle visits) and their
+  // hierarchies; each hierarchy's build is parallel inside
+  bool want[NSUB] = {false, false, false, false, false};
+  for (char ch : ams.cycle) {
+    const int sp = ams_subspace(ch);
+    if (sp >= 0) want[sp] = true;
+  }
+  HCsr nod[NSUB];
+  if (want[0] || want[1] || want[2] || want[3]) assemble_nodal(c, nod);
+  if (want[SUB_PIVEC]) assemble_pi_vector(c, nod[SUB_PIVEC], c.opt.pi_coupled != 0);
   AmgParams prm;
   prm.theta = c.opt.amg_theta;
   prm.pmax = c.opt.amg_pmax;
   prm.max_coarse = c.opt.amg_max_coarse;
   prm.max_levels = c.opt.amg_max_levels;
-  for (int sp = 0; sp < 4; ++sp) {
+  for (int sp = 0; sp < NSUB; ++sp) {
+    auto &S = ams.sub[sp];
+    S.lv.clear();
+    S.coarse = HCsr();
+    S.nc = 0;
+    S.cinv.release();
+    S.cinv_w.clear();
+    if (!want[sp]) continue;
     if (per_frequency) {
       for (size_t k = 0; k < nod[sp].vc.size(); ++k) nod[sp].vc[k] += w * nod[sp].vm[k];
       nod[sp].vm.clear();
     }
-  }
-  HostAmg hamg[4];
-#pragma omp parallel for schedule(dynamic, 1)
-  for (int sp = 0; sp < 4; ++sp) {
+    HostAmg hamg;
     AmgParams p2 = prm;
     p2.seed = prm.seed + 7919ull * (uint64_t)sp;
-    amg_build(nod[sp], w_ref, p2, hamg[sp]);
-  }
-  for (int sp = 0; sp < 4; ++sp) {
-    auto &S = ams.sub[sp];
-    S.lv.clear();
-    S.lv.resize(hamg[sp].lv.size());
-    for (size_t l = 0; l < hamg[sp].lv.size(); ++l) {
-      upload_csr(hamg[sp].lv[l].A, S.lv[l].A, true, s);
-      upload_csr(hamg[sp].lv[l].P, S.lv[l].P, false, s);
-      upload_csr(hamg[sp].lv[l].R, S.lv[l].R, false, s);
-      S.lv[l].nnzA = hamg[sp].lv[l].A.nnz();
-      S.lv[l].nnzP = hamg[sp].lv[l].P.nnz();
-      S.lv[l].nnzR = hamg[sp].lv[l].R.nnz();
+    p2.num_functions = sp == SUB_PIVEC ? 3 : 1;
+    amg_build(nod[sp], w_ref, p2, hamg);
+    S.lv.resize(hamg.lv.size());
+    for (size_t l = 0; l < hamg.lv.size(); ++l) {
+      upload_csr(hamg.lv[l].A, S.lv[l].A, true, s);
+      upload_csr(hamg.lv[l].P, S.lv[l].P, false, s);
+      upload_csr(hamg.lv[l].R, S.lv[l].R, false, s);
+      S.lv[l].nnzA = hamg.lv[l].A.nnz();
+      S.lv[l].nnzP = hamg.lv[l].P.nnz();
+      S.lv[l].nnzR = hamg.lv[l].R.nnz();
     }
-    S.coarse = std::move(hamg[sp].coarse);
+    S.coarse = std::move(hamg.coarse);
     S.nc = S.coarse.n;
-    S.cinv.release();
-    S.cinv_w.clear();
   }
-  for (int sp = 0; sp < 4; ++sp) {
+  for (int sp = 0; sp < NSUB; ++sp) {
     ams.wb[sp].clear();
     ams.wx[sp].clear();
     ams.wr[sp].clear();
     ams.wx2[sp].clear();
+    ams.wd[sp].clear();
   }
   ams.ws_K = 0;
 }
@@ -244,9 +255,9 @@ void Ams<T>::set_columns(const std::vector<double> &col_omega, cudaStream_t s) {
   const int *cs_before = cslot.p;
   cslot.upload(slot, s);
   if (cslot.p != cs_before) graphs.clear();
-  for (int sp = 0; sp < 4; ++sp) {
+  for (int sp = 0; sp < NSUB; ++sp) {
     Sub &S = sub[sp];
-    if (S.cinv_w == distinct && S.cinv.p) continue;
+    if (S.nc == 0 || (S.cinv_w == distinct && S.cinv.p)) continue;
     size_t nc2 = (size_t)S.nc * S.nc;
     std::vector<double> all(nc2 * distinct.size());
 #pragma omp parallel for schedule(dynamic, 1)
@@ -262,6 +273,7 @@ void Ams<T>::set_columns(const std::vector<double> &col_omega, cudaStream_t s) {
   }
   EMG_CUDA(cudaStreamSynchronize(s));
   ensure_workspace(s);
+  prepare_fused(s);
 }
 
 template <typename T>
@@ -273,7 +285,7 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
   ex2.alloc((size_t)ne * K);
   ed.alloc((size_t)ne * K);
   gtmp.alloc((size_t)nv * K);
-  for (int sp = 0; sp < 4; ++sp) {
+  for (int sp = 0; sp < NSUB; ++sp) {
     Sub &S = sub[sp];
     size_t L = S.lv.size();
     wb[sp].clear();
@@ -325,9 +337,68 @@ void Ams<T>::spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s) {
 }
 
 template <typename T>
-static void level_spmm(const DCsr<T> &A, long nnz, int K, int mode, const double *omega, double w, const T *x,
-                       const T *b, T *y, cudaStream_t s) {
+void Ams<T>::emit_spmm(const SpmmArgs &a, long nnz, const char *bin, cudaStream_t s) {
+  if (rec) {
+    FusedOp op;
+    std::memset(&op, 0, sizeof(op));
+    op.kind = FOP_SPMM;
+    op.nnz = nnz;
+    op.a = a;
+    rec->push_back(op);
+    return;
+  }
+  KernelProfiler &pf = profiler();
+  cudaEvent_t ev = nullptr;
+  if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(a.n, nnz, K, sizeof(T), a.vm != nullptr, a.mode), &ev);
+  spmm_nnz<T>(K, a, nnz, s);
+  if (pf.enabled) pf.end(bin, s, ev);
+}
+
+template <typename T>
+void Ams<T>::emit_jac0(int n, const T *b, const T *l1c, const T *l1m, double w, T *y, T *d, cudaStream_t s) {
+  if (rec) {
+    FusedOp op;
+    std::memset(&op, 0, sizeof(op));
+    op.kind = d ? FOP_JAC0_2 : FOP_JAC0;
+    op.a.n = n;
+    op.a.b = b;
+    op.a.l1c = l1c;
+    op.a.l1m = l1m;
+    op.a.omega = omega.p;
+    op.a.relax_w = w;
+    op.a.y = y;
+    op.a.d = d;
+    rec->push_back(op);
+    return;
+  }
+  if (d) jacobi0_2<T>(n, K, b, l1c, l1m, omega.p, w, y, d, s);
+  else jacobi0<T>(n, K, b, l1c, l1m, omega.p, w, y, s);
+}
+
+template <typename T>
+void Ams<T>::emit_coarse(int sp, const T *b, T *x, cudaStream_t s) {
+  Sub &S = sub[sp];
+  if (rec) {
+    if (S.nc == 0) return;
+    FusedOp op;
+    std::memset(&op, 0, sizeof(op));
+    op.kind = FOP_COARSE;
+    op.a.n = S.nc;
+    op.a.vc = S.cinv.p;
+    op.a.ci = cslot.p;
+    op.a.b = b;
+    op.a.y = x;
+    rec->push_back(op);
+    return;
+  }
+  coarse_apply<T>(S.nc, K, S.cinv.p, cslot.p, b, x, s);
+}
+
+template <typename T>
+static SpmmArgs level_args(const DCsr<T> &A, int mode, const double *omega, double w, const T *x, const T *b,
+                           T *y) {
   SpmmArgs a;
+  std::memset(&a, 0, sizeof(a));
   a.n = A.n;
   a.rp = A.rp.p;
   a.ci = A.ci.p;
@@ -341,12 +412,7 @@ static void level_spmm(const DCsr<T> &A, long nnz, int K, int mode, const double
   a.y = y;
   a.relax_w = w;
   a.mode = mode;
-  KernelProfiler &pf = profiler();
-  cudaEvent_t ev = nullptr;
-  const char *bin = sizeof(T) == 4 ? "spmm_nodal_fp32" : "spmm_nodal_fp64";
-  if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(A.n, nnz, K, sizeof(T), A.vm.p != nullptr, mode), &ev);
-  spmm_nnz<T>(K, a, nnz, s);
-  if (pf.enabled) pf.end(bin, s, ev);
+  return a;
 }
 
 // Chebyshev coefficients for degree 2 on D^-1 A with D the l1 row sums:
@@ -371,6 +437,7 @@ T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b,
   const T *l1m = edge ? (two ? B.l1m.p : nullptr) : A->l1m.p;
   auto run = [&](int mode, const T *x, const T *bb, T *y, T *r, T *d, double c1, double c2) {
     SpmmArgs a;
+    std::memset(&a, 0, sizeof(a));
     a.n = n;
     a.rp = edge ? brp : A->rp.p;
     a.ci = edge ? bci : A->ci.p;
@@ -388,15 +455,11 @@ T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b,
     a.d = d;
     a.c1 = c1;
     a.c2 = c2;
-    KernelProfiler &pf = profiler();
-    cudaEvent_t ev = nullptr;
-    if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(n, nnz, K, sizeof(T), a.vm != nullptr, mode), &ev);
-    spmm_nnz<T>(K, a, nnz, s);
-    if (pf.enabled) pf.end(bin, s, ev);
+    emit_spmm(a, nnz, bin, s);
   };
   if (!cheb) {
     if (zero_guess) {
-      jacobi0<T>(n, K, b, l1c, l1m, omega.p, relax_w, cur, s);
+      emit_jac0(n, b, l1c, l1m, relax_w, cur, nullptr, s);
       return cur;
     }
     run(SPMM_JAC, cur, b, oth, nullptr, nullptr, 0, 0);
@@ -404,7 +467,7 @@ T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b,
   }
   static const Cheb2 ch;
   if (zero_guess) {
-    jacobi0_2<T>(n, K, b, l1c, l1m, omega.p, ch.inv_theta, cur, dbuf, s);
+    emit_jac0(n, b, l1c, l1m, ch.inv_theta, cur, dbuf, s);
     run(SPMM_CHEB2, dbuf, nullptr, cur, const_cast<T *>(b), nullptr, ch.c1, ch.c2);
     return cur;
   }
@@ -417,8 +480,12 @@ template <typename T>
 void Ams<T>::vcycle(int sp, int l, cudaStream_t s) {
   Sub &S = sub[sp];
   const int L = (int)S.lv.size();
+  if (fused && !rec && l == fused_from[sp] && l < L) {
+    launch_fused(sp, s);
+    return;
+  }
   if (l == L) {
-    coarse_apply<T>(S.nc, K, S.cinv.p, cslot.p, wb[sp][l].p, wx[sp][l].p, s);
+    emit_coarse(sp, wb[sp][l].p, wx[sp][l].p, s);
     return;
   }
   Level &lv = S.lv[l];
@@ -436,14 +503,92 @@ void Ams<T>::vcycle(int sp, int l, cudaStream_t s) {
     T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, it == 0, bin, s);
     if (res != cur) std::swap(cur, oth);
   }
-  level_spmm<T>(lv.A, lv.nnzA, K, SPMM_RES, omega.p, relax_w, cur, b, r, s);
-  level_spmm<T>(lv.R, lv.nnzR, K, SPMM_AX, nullptr, 1.0, r, nullptr, wb[sp][l + 1].p, s);
+  emit_spmm(level_args<T>(lv.A, SPMM_RES, omega.p, relax_w, cur, b, r), lv.nnzA, bin, s);
+  emit_spmm(level_args<T>(lv.R, SPMM_AX, nullptr, 1.0, r, nullptr, wb[sp][l + 1].p), lv.nnzR, bin, s);
   vcycle(sp, l + 1, s);
-  level_spmm<T>(lv.P, lv.nnzP, K, SPMM_ADD, nullptr, 1.0, wx[sp][l + 1].p, nullptr, cur, s);
+  emit_spmm(level_args<T>(lv.P, SPMM_ADD, nullptr, 1.0, wx[sp][l + 1].p, nullptr, cur), lv.nnzP, bin, s);
   for (int it = 0; it < amg_relax_times; ++it) {
     T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, false, bin, s);
     if (res != cur) std::swap(cur, oth);
   }
+}
+
+template <typename T>
+void Ams<T>::prepare_fused(cudaStream_t s) {
+  if (!fused || (fused_epoch == graphs.epoch && ws_K == K)) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  EMG_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) fail(EMG_ERR_STATE, "fused V-cycle steps not recorded before capture");
+  ensure_workspace(s);
+  bool moved = false;
+  std::vector<FusedOp> lists[NSUB];  // alive until the uploads have completed
+  for (int sp = 0; sp < NSUB; ++sp) {
+    std::vector<FusedOp> &ops = lists[sp];
+    // levels below fused_rows rows run fused; the larger ones step by step
+    const int L = (int)sub[sp].lv.size();
+    int l0 = 0;
+    while (l0 < L && sub[sp].lv[l0].A.n >= fused_rows) ++l0;
+    fused_from[sp] = l0;
+    if (l0 >= L) {
+      fops_n[sp] = 0;
+      fops_bytes[sp] = 0;
+      continue;
+    }
+    rec = &ops;
+    try {
+      vcycle(sp, l0, s);
+    } catch (...) {
+      rec = nullptr;
+      throw;
+    }
+    rec = nullptr;
+    double bytes = 0;
+    for (const FusedOp &op : ops)
+      if (op.kind == FOP_SPMM) bytes += spmm_algo_bytes(op.a.n, op.nnz, K, sizeof(T), op.a.vm != nullptr, op.a.mode);
+    const FusedOp *before = fops[sp].p;
+    fops[sp].upload(ops, s);
+    moved |= fops[sp].p != before;
+    fops_n[sp] = (int)ops.size();
+    fops_bytes[sp] = bytes;
+  }
+  if (!fbar.p) {
+    fbar.alloc(2);
+    ferr.alloc(1);
+    moved = true;
+  }
+  fbar.zero(s);
+  ferr.zero(s);
+  if (!h_ferr.p) EMG_CUDA(cudaMallocHost((void **)&h_ferr.p, sizeof(int)));
+  *h_ferr.p = 0;
+  EMG_CUDA(cudaStreamSynchronize(s));  // host step lists go out of scope
+  if (moved) graphs.clear();           // captured graphs hold the old addresses
+  fused_epoch = graphs.epoch;
+}
+
+template <typename T>
+void Ams<T>::check_fused(cudaStream_t s) {
+  if (!h_ferr.p || *(volatile int *)h_ferr.p == 0) return;
+  fbar.zero(s);
+  ferr.zero(s);
+  EMG_CUDA(cudaStreamSynchronize(s));
+  *h_ferr.p = 0;
+  fail(EMG_ERR_CUDA, "fused nodal V-cycle: a grid barrier wait timed out");
+}
+
+template <typename T>
+void Ams<T>::run_vcycle(int sp, cudaStream_t s) {
+  if (fused && (fused_epoch != graphs.epoch || ws_K != K)) prepare_fused(s);
+  vcycle(sp, 0, s);
+}
+
+template <typename T>
+void Ams<T>::launch_fused(int sp, cudaStream_t s) {
+  KernelProfiler &pf = profiler();
+  cudaEvent_t ev = nullptr;
+  const char *bin = sizeof(T) == 4 ? "vcycle_fused_fp32" : "vcycle_fused_fp64";
+  if (pf.enabled) pf.begin(bin, s, fops_bytes[sp], &ev);
+  vcycle_fused<T>(K, fops[sp].p, fops_n[sp], fbar.p, ferr.p, fused_bps, s);
+  if (pf.enabled) pf.end(bin, s, ev);
 }
 
 // One AMS application.  With graphs enabled the first call for a (b, x) pair
@@ -454,6 +599,10 @@ template <typename T>
 void Ams<T>::apply(const T *b, T *x, cudaStream_t s) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   EMG_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (fused && cs == cudaStreamCaptureStatusNone) {
+    check_fused(s);
+    prepare_fused(s);
+  }
   if (!use_graphs || cs != cudaStreamCaptureStatusNone || profiler().enabled) {
     apply_eager(b, x, s);
     return;
@@ -511,8 +660,8 @@ void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
       }
       continue;
     }
-    int sp = ch == '1' ? 0 : (ch - '2');
-    if (sp < 0 || sp > 3) fail(EMG_ERR_OPTION, "bad AMS cycle character '%c'", ch);
+    const int sp = ams_subspace(ch);
+    if (sp < 0) fail(EMG_ERR_OPTION, "bad AMS cycle character '%c'", ch);
     const T *tg = sp == 0 ? nullptr : tangent.p;
     if (sp == 0) {
       // gradient space: G^T (b - B x) = G^T b - (G^T B) x
@@ -549,19 +698,20 @@ void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
       }
       ams_restrict<T>(nv, K, sp, inc_rp, inc, tg, er.p, wb[sp][0].p, s);
     }
-    vcycle(sp, 0, s);
+    run_vcycle(sp, s);
     // split form: the closing gradient correction stays a vertex potential
     // (wx[0][0]); the caller adds G phi in higher precision
     if (split_gradient && sp == 0 && ci + 1 == cycle.size()) continue;
     ams_prolong_add<T>(ne, K, sp, edges, tg, wx[sp][0].p, cur, s);
   }
   if (cur != x) EMG_CUDA(cudaMemcpyAsync(x, cur, sizeof(T) * (size_t)ne * K, cudaMemcpyDeviceToDevice, s));
+  if (fused && h_ferr.p) EMG_CUDA(cudaMemcpyAsync(h_ferr.p, ferr.p, sizeof(int), cudaMemcpyDeviceToHost, s));
 }
 
 template <typename T>
 size_t Ams<T>::device_bytes() const {
   size_t b = B.vc.bytes() + B.vm.bytes() + B.l1c.bytes() + B.l1m.bytes() + tangent.bytes();
-  for (int sp = 0; sp < 4; ++sp)
+  for (int sp = 0; sp < NSUB; ++sp)
     for (auto &l : sub[sp].lv)
       b += l.A.rp.bytes() + l.A.ci.bytes() + l.A.vc.bytes() + l.A.vm.bytes() + l.P.rp.bytes() + l.P.ci.bytes() +
            l.P.vc.bytes() + l.R.rp.bytes() + l.R.ci.bytes() + l.R.vc.bytes();

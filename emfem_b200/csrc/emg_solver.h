@@ -1,6 +1,7 @@
 // Solver engine: AMS preconditioner, batched FCG, batched FGMRES.
 #pragma once
 
+#include <algorithm>
 #include <functional>
 #include <map>
 #include <utility>
@@ -21,7 +22,8 @@ struct GraphCache {
   GraphCache() = default;
   GraphCache(const GraphCache &) = delete;
   GraphCache &operator=(const GraphCache &) = delete;
-  GraphCache(GraphCache &&o) noexcept : exec(std::move(o.exec)), seen(std::move(o.seen)), kernels(std::move(o.kernels)) {
+  GraphCache(GraphCache &&o) noexcept
+      : exec(std::move(o.exec)), seen(std::move(o.seen)), kernels(std::move(o.kernels)), epoch(o.epoch + 1) {
     o.exec.clear();
   }
   GraphCache &operator=(GraphCache &&o) noexcept {
@@ -30,18 +32,59 @@ struct GraphCache {
       exec = std::move(o.exec);
       seen = std::move(o.seen);
       kernels = std::move(o.kernels);
+      epoch = std::max(epoch, o.epoch) + 1;
       o.exec.clear();
     }
     return *this;
   }
   ~GraphCache() { clear(); }
+  long epoch = 0;  // bumped by every clear(): device addresses may have moved
   void clear() {
+    ++epoch;
     for (auto &kv : exec) cudaGraphExecDestroy(kv.second);
     exec.clear();
     seen.clear();
     kernels.clear();
   }
 };
+
+// one pinned host word (move-only)
+struct PinnedWord {
+  int *p = nullptr;
+  PinnedWord() = default;
+  PinnedWord(const PinnedWord &) = delete;
+  PinnedWord &operator=(const PinnedWord &) = delete;
+  PinnedWord(PinnedWord &&o) noexcept : p(o.p) { o.p = nullptr; }
+  PinnedWord &operator=(PinnedWord &&o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      o.p = nullptr;
+    }
+    return *this;
+  }
+  ~PinnedWord() { release(); }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+  }
+};
+
+// AMS subspaces: 0 = gradient G (cycle character '1'), 1..3 = Pi_x, Pi_y,
+// Pi_z as separate scalar spaces ('3', '4', '5'), 4 = the vector space Pi
+// with its coupled operator Pi^T B Pi ('2')
+constexpr int NSUB = 5;
+constexpr int SUB_PIVEC = 4;
+inline int ams_subspace(char ch) {
+  switch (ch) {
+  case '1': return 0;
+  case '2': return SUB_PIVEC;
+  case '3': return 1;
+  case '4': return 2;
+  case '5': return 3;
+  }
+  return -1;
+}
 
 // AMS (Hiptmair-Xu auxiliary space preconditioner, as hypre's AMS applies it)
 // for B(w) = C + w Ms on K real columns with per-column w.
@@ -62,7 +105,7 @@ struct Ams {
   const int *brp = nullptr, *bci = nullptr;
   long nnzB = 0;
   bool two = true;  // two value parts (batched) or combined (one frequency)
-  Sub sub[4];
+  Sub sub[NSUB];
   DBuf<T> tangent;
   // G^T B (vertex x edge): curl part (boundary elements only) and mass part
   const int *grp = nullptr, *gci = nullptr;
@@ -78,7 +121,21 @@ struct Ams {
   int cheb = 1;                    // 1: degree-2 Chebyshev smoothing, 0: l1-Jacobi
   bool use_graphs = true;          // replay each application as one CUDA graph
   bool split_gradient = false;     // last '1' of the cycle returned as potential gphi()
+  // each nodal V-cycle as one cooperative launch (emg_fused.cu) instead of
+  // its 40-70 step launches; the step lists are recorded from vcycle()
+  bool fused = false;
+  int fused_bps = 0;               // resident blocks per SM cap (0: occupancy limit)
+  int fused_rows = 1 << 30;        // levels with fewer rows run fused
+  int fused_from[NSUB] = {0, 0, 0, 0, 0};
   GraphCache graphs;
+  std::vector<FusedOp> *rec = nullptr;  // set while vcycle() records instead of launching
+  DBuf<FusedOp> fops[NSUB];
+  int fops_n[NSUB] = {0, 0, 0, 0, 0};
+  double fops_bytes[NSUB] = {0, 0, 0, 0, 0};
+  long fused_epoch = -1;           // graphs.epoch the step lists were recorded at
+  DBuf<unsigned> fbar;             // grid barrier words
+  DBuf<int> ferr;                  // barrier timeout flag (device)
+  PinnedWord h_ferr;               // pinned copy, refreshed after every application
   // per-call state
   int K = 0;
   DBuf<double> omega;              // K
@@ -86,7 +143,7 @@ struct Ams {
   std::vector<double> h_omega;
   // workspace
   DBuf<T> er, ex2, ed;
-  std::vector<DBuf<T>> wb[4], wx[4], wr[4], wx2[4], wd[4];
+  std::vector<DBuf<T>> wb[NSUB], wx[NSUB], wr[NSUB], wx2[NSUB], wd[NSUB];
 
   void set_columns(const std::vector<double> &col_omega, cudaStream_t s);
   void apply(const T *b, T *x, cudaStream_t s);
@@ -96,6 +153,18 @@ struct Ams {
   size_t device_bytes() const;
 
   void vcycle(int sp, int l, cudaStream_t s);
+  // runs subspace sp's V-cycle: the levels with at least fused_rows rows
+  // step by step, the rest as one fused launch
+  void run_vcycle(int sp, cudaStream_t s);
+  void launch_fused(int sp, cudaStream_t s);
+  // records the fused step lists for the current workspace (not while capturing)
+  void prepare_fused(cudaStream_t s);
+  // fails (and resets the barrier) when a fused launch reported a timeout
+  void check_fused(cudaStream_t s);
+  // step emitters: launch now, or append to *rec
+  void emit_spmm(const SpmmArgs &a, long nnz, const char *bin, cudaStream_t s);
+  void emit_jac0(int n, const T *b, const T *l1c, const T *l1m, double w, T *y, T *d, cudaStream_t s);
+  void emit_coarse(int sp, const T *b, T *x, cudaStream_t s);
   // one smoothing application on operator A (edge B when A == nullptr);
   // returns the buffer holding the result (cur, or oth after a swap)
   T *smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b, T *rbuf, T *dbuf, bool zero_guess,
