@@ -79,17 +79,29 @@ static inline double hash_unit(uint64_t x) {
 // PMIS: cf[i] = 1 (C) or -1 (F)
 static void pmis(int n, const std::vector<int> &srp, const std::vector<int> &sci, uint64_t seed,
                  std::vector<int> &cf) {
-  // transpose of S
+  // transpose of S (the order inside a row of S^T does not matter below)
   std::vector<int> trp(n + 1, 0), tci(sci.size());
-  for (size_t k = 0; k < sci.size(); ++k) trp[sci[k] + 1]++;
+  const long ns = (long)sci.size();
+#pragma omp parallel for schedule(static)
+  for (long k = 0; k < ns; ++k) {
+#pragma omp atomic
+    trp[sci[k] + 1]++;
+  }
   for (int i = 0; i < n; ++i) trp[i + 1] += trp[i];
   {
     std::vector<int> pos(trp.begin(), trp.end() - 1);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i)
-      for (int k = srp[i]; k < srp[i + 1]; ++k) tci[pos[sci[k]]++] = i;
+      for (int k = srp[i]; k < srp[i + 1]; ++k) {
+        int p;
+#pragma omp atomic capture
+        p = pos[sci[k]]++;
+        tci[p] = i;
+      }
   }
   std::vector<double> lam(n);
   cf.assign(n, 0);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; ++i) {
     int infl = trp[i + 1] - trp[i];
     lam[i] = infl + hash_unit(seed * 1000003ull + (uint64_t)i);
@@ -115,15 +127,28 @@ static void pmis(int n, const std::vector<int> &srp, const std::vector<int> &sci
       }
       newc[i] = best;
     }
-    for (int i : und)
-      if (newc[i]) cf[i] = 1;
-    // points that strongly depend on a new C point become F
-    for (int i : und)
-      if (newc[i]) {
-        newc[i] = 0;
-        for (int k = trp[i]; k < trp[i + 1]; ++k)
-          if (cf[tci[k]] == 0) cf[tci[k]] = -1;
+    const long nu = (long)und.size();
+#pragma omp parallel for schedule(static)
+    for (long u = 0; u < nu; ++u)
+      if (newc[und[u]]) cf[und[u]] = 1;
+    // points that strongly depend on a new C point become F (every writer
+    // stores the same -1 into a still-undecided point)
+#pragma omp parallel for schedule(static)
+    for (long u = 0; u < nu; ++u) {
+      const int i = und[u];
+      if (!newc[i]) continue;
+      newc[i] = 0;
+      for (int k = trp[i]; k < trp[i + 1]; ++k) {
+        const int j = tci[k];
+        int cj;
+#pragma omp atomic read
+        cj = cf[j];
+        if (cj == 0) {
+#pragma omp atomic write
+          cf[j] = -1;
+        }
       }
+    }
     std::vector<int> next;
     next.reserve(und.size());
     for (int i : und)
@@ -290,6 +315,79 @@ HCsr spgemm(const HCsr &A, const HCsr &B) {
   return C;
 }
 
+// Galerkin product C = R A P in one pass per coarse row (R, P single part,
+// A one or two parts): no intermediate A P, both value parts together.
+HCsr galerkin(const HCsr &R, const HCsr &A, const HCsr &P) {
+  HCsr C;
+  C.n = R.n;
+  C.m = P.m;
+  const bool two = !A.vm.empty();
+  std::vector<int> cnt(C.n + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<int> mark(P.m, -1);
+#pragma omp for schedule(dynamic, 64)
+    for (int I = 0; I < C.n; ++I) {
+      int c = 0;
+      for (int kr = R.rp[I]; kr < R.rp[I + 1]; ++kr) {
+        const int i = R.ci[kr];
+        for (int ka = A.rp[i]; ka < A.rp[i + 1]; ++ka) {
+          const int k = A.ci[ka];
+          for (int kp = P.rp[k]; kp < P.rp[k + 1]; ++kp)
+            if (mark[P.ci[kp]] != I) {
+              mark[P.ci[kp]] = I;
+              ++c;
+            }
+        }
+      }
+      cnt[I + 1] = c;
+    }
+  }
+  C.rp.assign(C.n + 1, 0);
+  for (int I = 0; I < C.n; ++I) C.rp[I + 1] = C.rp[I] + cnt[I + 1];
+  C.ci.resize(C.rp[C.n]);
+  C.vc.resize(C.rp[C.n]);
+  if (two) C.vm.resize(C.rp[C.n]);
+#pragma omp parallel
+  {
+    std::vector<int> mark(P.m, -1);
+    std::vector<double> ac(P.m), am(two ? P.m : 0);
+    std::vector<int> cols;
+#pragma omp for schedule(dynamic, 64)
+    for (int I = 0; I < C.n; ++I) {
+      cols.clear();
+      for (int kr = R.rp[I]; kr < R.rp[I + 1]; ++kr) {
+        const int i = R.ci[kr];
+        const double r = R.vc[kr];
+        for (int ka = A.rp[i]; ka < A.rp[i + 1]; ++ka) {
+          const int k = A.ci[ka];
+          const double rc = r * A.vc[ka], rm = two ? r * A.vm[ka] : 0.0;
+          for (int kp = P.rp[k]; kp < P.rp[k + 1]; ++kp) {
+            const int J = P.ci[kp];
+            if (mark[J] != I) {
+              mark[J] = I;
+              ac[J] = 0;
+              if (two) am[J] = 0;
+              cols.push_back(J);
+            }
+            ac[J] += rc * P.vc[kp];
+            if (two) am[J] += rm * P.vc[kp];
+          }
+        }
+      }
+      std::sort(cols.begin(), cols.end());
+      int p = C.rp[I];
+      for (int J : cols) {
+        C.ci[p] = J;
+        C.vc[p] = ac[J];
+        if (two) C.vm[p] = am[J];
+        ++p;
+      }
+    }
+  }
+  return C;
+}
+
 void amg_build(const HCsr &A0, double w_ref, const AmgParams &prm, HostAmg &out) {
   out.lv.clear();
   HCsr A = A0;
@@ -314,23 +412,7 @@ void amg_build(const HCsr &A0, double w_ref, const AmgParams &prm, HostAmg &out)
       fn.swap(fc);
     }
     HCsr R = transpose(P);
-    HCsr AP = spgemm(A, P);
-    HCsr RAP;
-    {
-      // R * AP with AP two-part: form both parts via the single-part B path
-      HCsr APc = AP;
-      APc.vm.clear();
-      HCsr Rc = R;
-      HCsr Cc = spgemm(Rc, APc);
-      if (!AP.vm.empty()) {
-        HCsr APm = AP;
-        APm.vc = AP.vm;
-        APm.vm.clear();
-        HCsr Cm = spgemm(Rc, APm);
-        Cc.vm = Cm.vc;
-      }
-      RAP = std::move(Cc);
-    }
+    HCsr RAP = galerkin(R, A, P);
     HostLevel L;
     L.A = std::move(A);
     L.P = std::move(P);

@@ -98,7 +98,8 @@ void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
 // launchers defined in emg_estimate.cu
 void launch_estimate(Context &c, double omega, int nsol, const double *const *sol_dev, double *eta_dev,
                      double *err_dev, double *scratch_vol, double *scratch_fe);
-void launch_rhs_mt(Context &c, int k, const double *omega_dev, const double *bv_dev, double *s_dev);
+void launch_rhs_mt(Context &c, int k, const double *omega_dev, const double *bv_dev, const int *brank_dev,
+                   double *s_dev);
 
 struct Workspace {
   Fcg<double> fcg64;
@@ -222,13 +223,19 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_fused_blocks_per_sm") o.fused_bps = geti(k, v);
     else if (key == "emg_fused_rows") o.fused_rows = geti(k, v);
     else if (key == "emg_pi_coupled") o.pi_coupled = v.empty() ? 1 : getb(v);
+    else if (key == "emg_block_inner_rtol") o.block_inner_rtol = getr(k, v);
+    else if (key == "emg_block_inner_max_it") o.block_inner_max_it = geti(k, v);
+    else if (key == "emg_block_fcg_mmax") o.block_fcg_mmax = geti(k, v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
     else if (key.rfind("A_", 0) == 0 || key.rfind("B_", 0) == 0) ignored.push_back(k);
     else fail(EMG_ERR_OPTION, "unknown option %s", k.c_str());
   }
   if (o.gmres_restart < 1 || o.gmres_restart > 32) fail(EMG_ERR_OPTION, "A_ksp_gmres_restart must be in [1, 32]");
-  if (o.fcg_mmax < 1 || o.fcg_mmax > 30) fail(EMG_ERR_OPTION, "B_ksp_fcg_mmax must be in [1, 30]");
+  if (o.fcg_mmax < 1 || o.fcg_mmax > 30 || o.block_fcg_mmax < 1 || o.block_fcg_mmax > 30)
+    fail(EMG_ERR_OPTION, "FCG truncation lengths must be in [1, 30]");
   if (o.ams_relax_times < 1 || o.amg_relax_times < 1) fail(EMG_ERR_OPTION, "relax times must be >= 1");
+  if (o.inner_max_it < 1 || o.block_inner_max_it < 1) fail(EMG_ERR_OPTION, "inner iteration caps must be >= 1");
+  if (!(o.inner_rtol > 0) || !(o.block_inner_rtol > 0)) fail(EMG_ERR_OPTION, "inner tolerances must be > 0");
 }
 
 // ---------------------------------------------------------------------------
@@ -427,7 +434,8 @@ static void mt_boundary_geometry(Context &c, const std::vector<unsigned char> &b
 
 // boundary DOF values of one (frequency, polarisation): the 1-D plane-wave
 // field of the four corner soundings at each distinct depth, blended per edge
-static void boundary_values(Context &c, const MtBoundary &g, double freq, int mode, std::vector<std::complex<double>> &bv) {
+static void boundary_values(Context &c, const MtBoundary &g, double freq, int mode,
+                            std::vector<std::complex<double>> &bv) {  // bv[b]: value of edge g.edge[b]
   typedef std::complex<double> zc;
   PlaneWave1D pw[4];
   for (int q = 0; q < 4; ++q) pw[q].init(&c.bg_ztop[q * c.bg_maxl], &c.bg_lsig[q * c.bg_maxl], c.bg_nlay[q], freq);
@@ -442,7 +450,7 @@ static void boundary_values(Context &c, const MtBoundary &g, double freq, int mo
       pw[q].field(g.zs[iz], eh);
       f[4 * (size_t)iz + q] = std::conj(eh[comp]);
     }
-  bv.assign(c.ne, zc(0));
+  bv.assign(nb, zc(0));
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nb; ++b) {
     const double *co = &g.co[4 * (size_t)b];
@@ -452,7 +460,7 @@ static void boundary_values(Context &c, const MtBoundary &g, double freq, int mo
     const double ed0 = g.ed[2 * (size_t)b], ed1 = g.ed[2 * (size_t)b + 1];
     zc num = ed0 * ep[0] + ed1 * ep[1];
     zc dof = num / g.den[b];
-    bv[g.edge[b]] = std::abs(dof) > 1E-13 ? dof : zc(0.0);
+    bv[b] = std::abs(dof) > 1E-13 ? dof : zc(0.0);
   }
 }
 
@@ -573,6 +581,9 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_fused_blocks_per_sm") *value = o.fused_bps;
   else if (k == "emg_fused_rows") *value = o.fused_rows;
   else if (k == "emg_pi_coupled") *value = o.pi_coupled;
+  else if (k == "emg_block_inner_rtol") *value = o.block_inner_rtol;
+  else if (k == "emg_block_inner_max_it") *value = o.block_inner_max_it;
+  else if (k == "emg_block_fcg_mmax") *value = o.block_fcg_mmax;
   else fail(EMG_ERR_OPTION, "unknown option %s", key);
   EMG_API_END
 }
@@ -604,6 +615,7 @@ int emg_set_mesh(emg_context *c, int nv, const double *pts, int nt, const int *t
   c->h_nbr.assign(nbr, nbr + 4L * nt);
   c->h_non.assign(non, non + 4L * nt);
   c->h_ebdr.assign(ebdr, ebdr + ne);
+  c->bnd_rank.release();
   c->pts.upload(c->h_pts, c->stream);
   c->tets.upload(c->h_tets, c->stream);
   c->attr.upload(c->h_attr, c->stream);
@@ -913,22 +925,34 @@ static void rhs_mt_block(Context &c, int k, const double *freqs, const int *mode
   std::vector<unsigned char> bdr(c.nt);
   c.bdr_cell.download(bdr.data(), c.nt, c.stream);
   EMG_CUDA(cudaStreamSynchronize(c.stream));
-  std::vector<double> bv((size_t)c.ne * k * 2, 0.0), om(k);
+  // boundary values travel compact: row r = rank of the edge among the
+  // boundary edges (edge_bdr_marker order), k complex columns per row
+  if (c.bnd_rank.n != (size_t)c.ne) {
+    std::vector<int> rank(c.ne, -1);
+    int r = 0;
+    for (int e = 0; e < c.ne; ++e)
+      if (c.h_ebdr[e]) rank[e] = r++;
+    c.n_bnd = r;
+    c.h_bnd_rank = rank;
+    c.bnd_rank.upload(rank, c.stream);
+  }
   MtBoundary g;
   mt_boundary_geometry(c, bdr, g);
+  std::vector<double> bv((size_t)std::max(c.n_bnd, 1) * k * 2, 0.0), om(k);
   for (int j = 0; j < k; ++j) {
     std::vector<std::complex<double>> v;
     boundary_values(c, g, freqs[j], modes[j], v);
 #pragma omp parallel for schedule(static)
-    for (int e = 0; e < c.ne; ++e) {
-      bv[2 * ((size_t)e * k + j)] = v[e].real();
-      bv[2 * ((size_t)e * k + j) + 1] = v[e].imag();
+    for (int b = 0; b < (int)g.edge.size(); ++b) {
+      const size_t r = (size_t)c.h_bnd_rank[g.edge[b]];
+      bv[2 * (r * k + j)] = v[b].real();
+      bv[2 * (r * k + j) + 1] = v[b].imag();
     }
     om[j] = 2 * PI * freqs[j];
   }
   w.bvals.upload(bv, c.stream);
   w.omega_k.upload(om, c.stream);
-  launch_rhs_mt(c, k, w.omega_k.p, w.bvals.p, s_dev);
+  launch_rhs_mt(c, k, w.omega_k.p, w.bvals.p, c.bnd_rank.p, s_dev);
   EMG_CUDA(cudaStreamSynchronize(c.stream));
 }
 
@@ -1168,8 +1192,10 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     w.block_ready64 = true;
   }
   c.kernel_ms["block_setup"] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  auto tc = std::chrono::steady_clock::now();
   if (fp32) w.bams32.set_columns(col, c.stream);
   else w.bams64.set_columns(col, c.stream);
+  c.kernel_ms["setup_columns"] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc).count();
   // b = conj(s): the real-form system equals (C + i w Ms) z = conj(s)
   w.vec_a.alloc((size_t)n * k * 2);
   conj_copy_kernel<<<(unsigned)(((long)n * k + 255) / 256), 256, 0, c.stream>>>((long)n * k, (const double2 *)rhs_dev,
@@ -1178,7 +1204,7 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
   w.gm.k = k;
   w.gm.restart = o.restart > 0 ? o.restart : c.opt.gmres_restart;
   w.gm.omega.upload(om, c.stream);
-  w.fcg64.mmax = w.fcg32.mmax = c.opt.fcg_mmax;
+  w.fcg64.mmax = w.fcg32.mmax = c.opt.block_fcg_mmax;
   w.fcg64.verbose = w.fcg32.verbose = c.opt.verbose > 1;
   w.fcg64.total_its = w.fcg32.total_its = 0;
   if (fp32) {
@@ -1218,7 +1244,7 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     KernelProfiler &pf = profiler();
     cudaEvent_t ph = nullptr;
     if (pf.phases) pf.begin("phase_ams", c.stream, 0, &ph);
-    cvt_d2f((long)n * K2, r_, w.f_in.p, c.stream);
+    (void)r_;  // w.f_in holds (float) r_: the FCG update writes it
     w.bams32.apply(w.f_in.p, w.f_out.p, c.stream);
     add_gradient_f2d(n, K2, c.edges.p, w.f_out.p, w.bams32.gphi(), z_, c.stream);
     if (pf.phases) pf.end("phase_ams", c.stream, ph);
@@ -1227,8 +1253,10 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     KernelProfiler &pf = profiler();
     cudaEvent_t ph = nullptr;
     if (pf.phases) pf.begin("phase_fcg", c.stream, 0, &ph);
-    if (fp32) w.fcg64.solve_with(n, K2, pc32, opB64, v, z, c.opt.inner_rtol, c.opt.inner_max_it, c.stream);
-    else w.fcg64.solve(w.bams64, v, z, c.opt.inner_rtol, c.opt.inner_max_it, c.stream);
+    if (fp32)
+      w.fcg64.solve_with(n, K2, pc32, opB64, v, z, c.opt.block_inner_rtol, c.opt.block_inner_max_it, c.stream,
+                         w.f_in.p);
+    else w.fcg64.solve(w.bams64, v, z, c.opt.block_inner_rtol, c.opt.block_inner_max_it, c.stream);
     if (pf.phases) pf.end("phase_fcg", c.stream, ph);
   };
   SolveStats st;

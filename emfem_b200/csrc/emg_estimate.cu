@@ -288,7 +288,8 @@ struct LiftIn {
 };
 
 __global__ void __launch_bounds__(128) rhs_mt_kernel(LiftIn in, int nt, int k, const double *__restrict__ omega,
-                                                     const double2 *__restrict__ bv, double *__restrict__ s) {
+                                                     const double2 *__restrict__ bv, const int *__restrict__ brank,
+                                                     double *__restrict__ s) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt || !__ldg(in.bdr_cell + t)) return;
   TetGeom g;
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(128) rhs_mt_kernel(LiftIn in, int nt, int k, c
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
       if (!bd[i]) continue;
-      double2 v = __ldg(bv + (long)g.ge[i] * k + j);
+      double2 v = __ldg(bv + (long)__ldg(brank + g.ge[i]) * k + j);
       double cii = vc * (cu[i][0] * cu[i][0] + cu[i][1] * cu[i][1] + cu[i][2] * cu[i][2]);
       br[i] += v.x * cii;
       bi[i] += -v.y * cii;
@@ -351,11 +352,12 @@ __global__ void __launch_bounds__(128) rhs_mt_kernel(LiftIn in, int nt, int k, c
   }
 }
 
-void launch_rhs_mt(Context &c, int k, const double *omega_dev, const double *bv_dev, double *s_dev) {
+void launch_rhs_mt(Context &c, int k, const double *omega_dev, const double *bv_dev, const int *brank_dev,
+                   double *s_dev) {
   LiftIn in{c.pts.p, c.ctet.p, c.cedge.p, c.attr.p, c.cpar.p, c.ebdr.p, c.bdr_cell.p, c.sigma_tab.p};
   EMG_CUDA(cudaMemsetAsync(s_dev, 0, sizeof(double) * 2 * (size_t)c.ne * k, c.stream));
   rhs_mt_kernel<<<(unsigned)((c.nt + 127) / 128), 128, 0, c.stream>>>(in, c.nt, k, omega_dev, (const double2 *)bv_dev,
-                                                                      s_dev);
+                                                                      brank_dev, s_dev);
   EMG_LAUNCH_CHECK();
 }
 

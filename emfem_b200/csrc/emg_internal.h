@@ -146,7 +146,7 @@ struct Options {
   int inner_max_it = 100;
   int fcg_mmax = 1;
   std::string ams_cycle = "034515430";  // cycle type 13
-  std::string fp32_cycle = "034501";    // cycle of the FP32 AMS (gradient last)
+  std::string fp32_cycle = "0201";      // cycle of the FP32 AMS (gradient last)
   int ams_relax_times = 1;
   double ams_relax_weight = 1.0;
   double amg_theta = 0.25;
@@ -161,7 +161,12 @@ struct Options {
   int ams_fused = 0;          // small nodal levels as one cooperative launch per V-cycle
   int fused_bps = 0;          // its resident blocks per SM cap (0: occupancy limit)
   int fused_rows = 1 << 30;   // levels below this many rows run fused
-  int pi_coupled = 1;         // vector Pi space with (1) or without (0) its x/y/z couplings
+  int pi_coupled = 0;         // vector Pi space with (1) or without (0) its x/y/z couplings
+  // inner FCG of the batched path (emg_solve_block): a capped iteration count
+  // per outer step; the flexible outer Krylov absorbs the inexactness
+  double block_inner_rtol = 1e-2;
+  int block_inner_max_it = 30;
+  int block_fcg_mmax = 2;
   int verbose = 0;
 };
 
@@ -219,6 +224,10 @@ struct Context {
   std::map<int, DBuf<double>> sol;
   // timing
   std::map<std::string, double> kernel_ms;
+  // rank of each boundary edge among the boundary edges (-1 elsewhere)
+  std::vector<int> h_bnd_rank;
+  DBuf<int> bnd_rank;
+  int n_bnd = 0;
   std::unique_ptr<Workspace> ws;
   Context();
   ~Context();

@@ -236,7 +236,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) fcg_update_kernel(long total, int K, const double *__restrict__ alpha,
                                                          const T *__restrict__ p, const T *__restrict__ sv,
                                                          T *__restrict__ x, T *__restrict__ r,
-                                                         double *__restrict__ rn) {
+                                                         double *__restrict__ rn, float *__restrict__ r32) {
   __shared__ double sh[256];
   double acc = 0;
   const int c = threadIdx.x % K;
@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(256) fcg_update_kernel(long total, int K, cons
     T ri = r[i] - (T)al * sv[i];
     x[i] = xi;
     r[i] = ri;
+    if (r32) r32[i] = (float)ri;
     acc += (double)ri * (double)ri;
   }
   sh[threadIdx.x] = acc;
@@ -259,9 +260,9 @@ __global__ void __launch_bounds__(256) fcg_update_kernel(long total, int K, cons
 
 template <typename T>
 void fcg_update(int n, int K, const double *alpha, const T *p, const T *sv, T *x, T *r, double *rn,
-                cudaStream_t s) {
+                cudaStream_t s, float *r32) {
   long total = (long)n * K;
-  fcg_update_kernel<T><<<red_grid(total), 256, 0, s>>>(total, K, alpha, p, sv, x, r, rn);
+  fcg_update_kernel<T><<<red_grid(total), 256, 0, s>>>(total, K, alpha, p, sv, x, r, rn, r32);
   EMG_LAUNCH_CHECK();
 }
 
@@ -689,7 +690,7 @@ void cnorm2(int n, int K, const double *x, double *out, cudaStream_t s) {
   template void coldot<T>(int, int, const T *, const T *, double *, cudaStream_t);                              \
   template void coldot3<T>(int, int, const T *, const T *, const T *, const T *, const T *, const T *, double *,  \
                            cudaStream_t);                                                                        \
-  template void fcg_update<T>(int, int, const double *, const T *, const T *, T *, T *, double *, cudaStream_t); \
+  template void fcg_update<T>(int, int, const double *, const T *, const T *, T *, T *, double *, cudaStream_t, float *); \
   template void fcg_direction<T>(int, int, const T *, int, T *const *, const double *, T *, cudaStream_t);       \
   template void jacobi0<T>(int, int, const T *, const T *, const T *, const double *, double, T *, cudaStream_t); \
   template void jacobi0_2<T>(int, int, const T *, const T *, const T *, const double *, double, T *, T *,           \

@@ -39,9 +39,10 @@ void coldot(int n, int K, const T *a, const T *b, double *out, cudaStream_t s);
 template <typename T>
 void coldot3(int n, int K, const T *a1, const T *b1, const T *a2, const T *b2, const T *a3, const T *b3,
              double *out, cudaStream_t s);
-// x += alpha_c p ; r -= alpha_c s ; rn[c] += ||r_c||^2
+// x += alpha_c p ; r -= alpha_c s ; rn[c] += ||r_c||^2 ; r32 = (float) r when given
 template <typename T>
-void fcg_update(int n, int K, const double *alpha, const T *p, const T *sv, T *x, T *r, double *rn, cudaStream_t s);
+void fcg_update(int n, int K, const double *alpha, const T *p, const T *sv, T *x, T *r, double *rn, cudaStream_t s,
+                float *r32 = nullptr);
 // p = z - sum_j beta[j*K+c] * P_j  (nprev directions, pointers in a device array)
 template <typename T>
 void fcg_direction(int n, int K, const T *z, int nprev, T *const *Pj, const double *beta, T *p, cudaStream_t st);

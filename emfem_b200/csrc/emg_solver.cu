@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -96,9 +97,46 @@ static void upload_csr(const HCsr &h, DCsr<T> &d, bool with_l1, cudaStream_t s) 
 // ---------------------------------------------------------------------------
 // AMS setup
 // ---------------------------------------------------------------------------
+// Vector nodal operator without couplings: row 3 v + d of out is row v of
+// comp[d] with columns 3 u + d (comp[0..2] share one vertex pattern).
+static void interleave_components(const HCsr *comp, HCsr &out) {
+  const int nv = comp[0].n;
+  const bool two = !comp[0].vm.empty();
+  out.n = out.m = 3 * nv;
+  out.rp.assign(3 * (size_t)nv + 1, 0);
+  for (int v = 0; v < nv; ++v)
+    for (int d = 0; d < 3; ++d) out.rp[3 * v + d + 1] = comp[d].rp[v + 1] - comp[d].rp[v];
+  for (int i = 0; i < 3 * nv; ++i) out.rp[i + 1] += out.rp[i];
+  out.ci.resize(out.rp[3 * nv]);
+  out.vc.resize(out.rp[3 * nv]);
+  out.vm.resize(two ? out.rp[3 * nv] : 0);
+#pragma omp parallel for schedule(static)
+  for (int v = 0; v < nv; ++v)
+    for (int d = 0; d < 3; ++d) {
+      long p = out.rp[3 * v + d];
+      for (int k = comp[d].rp[v]; k < comp[d].rp[v + 1]; ++k, ++p) {
+        out.ci[p] = 3 * comp[d].ci[k] + d;
+        out.vc[p] = comp[d].vc[k];
+        if (two) out.vm[p] = comp[d].vm[k];
+      }
+    }
+}
+// host wall time of a setup stage, kept in the context's timing table
+struct StageClock {
+  Context &c;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  explicit StageClock(Context &cc) : c(cc) {}
+  void lap(const char *name) {
+    auto now = std::chrono::steady_clock::now();
+    c.kernel_ms[name] = std::chrono::duration<double, std::milli>(now - t).count();
+    t = now;
+  }
+};
+
 template <typename T>
 void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_ref) {
   cudaStream_t s = c.stream;
+  StageClock clk(c);
   ams.ne = c.ne;
   ams.nv = c.nv;
   ams.edges = c.edges.p;
@@ -159,6 +197,8 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
     ams.tangent.upload(tg, s);
     EMG_CUDA(cudaStreamSynchronize(s));
   }
+  EMG_CUDA(cudaStreamSynchronize(s));
+  clk.lap("setup_edge");
   // G^T B for the gradient-space residual
   {
     DBuf<double> gc, gm;
@@ -186,9 +226,16 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
     const int sp = ams_subspace(ch);
     if (sp >= 0) want[sp] = true;
   }
+  clk.lap("setup_gtb");
   HCsr nod[NSUB];
-  if (want[0] || want[1] || want[2] || want[3]) assemble_nodal(c, nod);
-  if (want[SUB_PIVEC]) assemble_pi_vector(c, nod[SUB_PIVEC], c.opt.pi_coupled != 0);
+  const bool pi_coupled = c.opt.pi_coupled != 0;
+  if (want[0] || want[1] || want[2] || want[3] || (want[SUB_PIVEC] && !pi_coupled)) assemble_nodal(c, nod);
+  if (want[SUB_PIVEC]) {
+    if (pi_coupled) assemble_pi_vector(c, nod[SUB_PIVEC], true);
+    else interleave_components(nod + 1, nod[SUB_PIVEC]);  // the x/y/z operators side by side
+  }
+  clk.lap("setup_nodal");
+  double amg_ms = 0, upload_ms = 0;
   AmgParams prm;
   prm.theta = c.opt.amg_theta;
   prm.pmax = c.opt.amg_pmax;
@@ -210,7 +257,10 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
     AmgParams p2 = prm;
     p2.seed = prm.seed + 7919ull * (uint64_t)sp;
     p2.num_functions = sp == SUB_PIVEC ? 3 : 1;
+    auto ta = std::chrono::steady_clock::now();
     amg_build(nod[sp], w_ref, p2, hamg);
+    auto tb = std::chrono::steady_clock::now();
+    amg_ms += std::chrono::duration<double, std::milli>(tb - ta).count();
     S.lv.resize(hamg.lv.size());
     for (size_t l = 0; l < hamg.lv.size(); ++l) {
       upload_csr(hamg.lv[l].A, S.lv[l].A, true, s);
@@ -222,7 +272,10 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
     }
     S.coarse = std::move(hamg.coarse);
     S.nc = S.coarse.n;
+    upload_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
   }
+  c.kernel_ms["setup_amg"] = amg_ms;
+  c.kernel_ms["setup_upload"] = upload_ms;
   for (int sp = 0; sp < NSUB; ++sp) {
     ams.wb[sp].clear();
     ams.wx[sp].clear();
@@ -731,7 +784,7 @@ int Fcg<T>::solve(Ams<T> &ams, const T *b, T *x, double rtol, int maxit, cudaStr
 template <typename T>
 int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> &pc,
                        const std::function<void(const T *, T *)> &opB, const T *b, T *x, double rtol, int maxit,
-                       cudaStream_t s) {
+                       cudaStream_t s, float *r32) {
   K = Kc;
   const size_t N = (size_t)n * K;
   if (mmax < 1) mmax = 1;
@@ -759,6 +812,10 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
   its.assign(K, 0);
   fill_zero<T>((long)N, x, s);
   EMG_CUDA(cudaMemcpyAsync(r.p, b, sizeof(T) * N, cudaMemcpyDeviceToDevice, s));
+  if (r32) {
+    if (sizeof(T) != 8) fail(EMG_ERR_STATE, "FP32 residual copy needs FP64 recurrences");
+    cvt_d2f((long)N, reinterpret_cast<const double *>(b), r32, s);
+  }
   bn.zero(s);
   coldot<T>(n, K, b, b, bn.p, s);
   std::vector<double> hbn(K), hrn(K);
@@ -804,7 +861,7 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
     fcg_alpha_kernel<<<(K + 63) / 64, 64, 0, s>>>(K, dots.p, eta.p + (size_t)head * K, act.p, alpha.p);
     EMG_LAUNCH_CHECK();
     rn.zero(s);
-    fcg_update<T>(n, K, alpha.p, p, sv, x, r.p, rn.p, s);
+    fcg_update<T>(n, K, alpha.p, p, sv, x, r.p, rn.p, s, r32);
     head = (head + 1) % mmax;
     nprev = std::min(nprev + 1, mmax);
     rn.download(hrn.data(), K, s);

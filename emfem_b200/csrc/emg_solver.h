@@ -198,9 +198,10 @@ struct Fcg {
   int solve(Ams<T> &ams, const T *b, T *x, double rtol, int maxit, cudaStream_t s);
   // generic form: pc(r, z) applies the preconditioner, opB(p, s) the operator;
   // n rows, K columns
+  // r32: when given, kept equal to (float) r for an FP32 preconditioner
   int solve_with(int n, int Kc, const std::function<void(const T *, T *)> &pc,
                  const std::function<void(const T *, T *)> &opB, const T *b, T *x, double rtol, int maxit,
-                 cudaStream_t s);
+                 cudaStream_t s, float *r32 = nullptr);
 };
 
 struct SolveStats {

@@ -14,10 +14,12 @@ A hierarchy coarsened to 16 rows (emg_amg_max_coarse) gives every nodal
 subspace several levels even on this small mesh.
 
 2. The vector Pi space (cycle character '2': Pi^T B Pi with its x/y/z
-couplings, systems AMG with the unknown approach), as hypre's cycle types
-1/3/5/7 use it, in the FP32 block cycle "0201" and the FP64 reference-facing
-solve: both converge to rtol 1e-10 and agree with the exact discrete solution
-(sparse direct solve) to 1e-6 of its largest entry.
+couplings and systems AMG with the unknown approach as hypre's cycle types
+1/3/5/7 use it, or its three diagonal blocks side by side), in the FP32 block
+cycle and the FP64 reference-facing solve, and the component cycle "034501"
+with the inner iteration cap of the reference: every variant converges to
+rtol 1e-10 and agrees with the exact discrete solution (sparse direct solve)
+to 1e-6 of its largest entry.
 """
 
 import numpy as np
@@ -80,7 +82,9 @@ def _direct(rp, ci, Cv, Mv, sr, si):
     return sla.spsolve(A, sr - 1j * si)
 
 
-@pytest.mark.parametrize("extra", ["-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 1",
+@pytest.mark.parametrize("extra", ["-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 1 -emg_pi_coupled 1",
+                                   "-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 3 -emg_pi_coupled 0",
+                                   "-emg_fp32_cycle 034501 -emg_block_inner_max_it 100",
                                    "-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 7 -emg_fused_vcycle 1 "
                                    "-emg_fused_rows 400"])
 def test_pi_vector_space_cycles(mt_small, extra):
