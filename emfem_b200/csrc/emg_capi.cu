@@ -1181,7 +1181,7 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     lg += std::log(om[j]);
   }
   const double wref = std::exp(lg / k);
-  const bool fp32 = o.inner_fp32 != 0;
+  const bool fp32 = o.inner_fp32 < 0 ? c.opt.inner_fp32 != 0 : o.inner_fp32 != 0;
   auto t0 = std::chrono::steady_clock::now();
   if (fp32 && !w.block_ready32) {
     ams_setup<float>(c, w.bams32, false, 0.0, wref);

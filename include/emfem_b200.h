@@ -180,7 +180,7 @@ typedef struct emg_block_opts {
   double rtol;           /* outer relative residual target (1e-8)           */
   int max_it;            /* outer iteration cap per column                   */
   int use_guess;         /* 1: x is the initial guess                        */
-  int inner_fp32;        /* 1: FP32 inner solve, 0: FP64                     */
+  int inner_fp32;        /* 1: FP32 AMS, 0: FP64, -1: -emg_inner_precision */
   int restart;           /* FGMRES restart (30)                              */
 } emg_block_opts;
 
