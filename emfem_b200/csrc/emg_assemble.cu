@@ -582,6 +582,7 @@ void assemble_pi_vector(Context &c, HCsr &out, bool coupled) {
 // B x is evaluated in FP32.
 // ---------------------------------------------------------------------------
 void build_gtb_pattern(Context &c) {
+  c.tiles.clear();
   const int nv = c.nv, nt = c.nt;
   std::vector<int> v2t_rp(nv + 1, 0), v2t;
   for (int t = 0; t < nt; ++t)

@@ -226,6 +226,8 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_block_inner_rtol") o.block_inner_rtol = getr(k, v);
     else if (key == "emg_block_inner_max_it") o.block_inner_max_it = geti(k, v);
     else if (key == "emg_block_fcg_mmax") o.block_fcg_mmax = geti(k, v);
+    else if (key == "emg_spmm_tiled") o.spmm_tiled = v.empty() ? 1 : getb(v);
+    else if (key == "emg_tiled_smem_kb") o.tiled_smem_kb = geti(k, v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
     else if (key.rfind("A_", 0) == 0 || key.rfind("B_", 0) == 0) ignored.push_back(k);
     else fail(EMG_ERR_OPTION, "unknown option %s", k.c_str());
@@ -236,6 +238,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
   if (o.ams_relax_times < 1 || o.amg_relax_times < 1) fail(EMG_ERR_OPTION, "relax times must be >= 1");
   if (o.inner_max_it < 1 || o.block_inner_max_it < 1) fail(EMG_ERR_OPTION, "inner iteration caps must be >= 1");
   if (!(o.inner_rtol > 0) || !(o.block_inner_rtol > 0)) fail(EMG_ERR_OPTION, "inner tolerances must be > 0");
+  if (o.tiled_smem_kb < 4 || o.tiled_smem_kb > 227) fail(EMG_ERR_OPTION, "emg_tiled_smem_kb must be in [4, 227]");
 }
 
 // ---------------------------------------------------------------------------
@@ -351,6 +354,23 @@ struct PlaneWave1D {
 
 // calculate_boundary_values (src/em_fwd.cc:402-486): Dirichlet value of every
 // boundary edge (first encounter in ascending tet order wins)
+const TiledPattern *tiled_pattern(Context &c, const int *rp_dev, const std::vector<int> &h_rp,
+                                  const std::vector<int> &h_ci, int row_bytes) {
+  if (!c.opt.spmm_tiled || h_rp.size() < 2) return nullptr;
+  const auto key = std::make_pair(rp_dev, row_bytes);
+  auto it = c.tiles.find(key);
+  if (it != c.tiles.end()) return it->second.get();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  EMG_CUDA(cudaStreamIsCapturing(c.stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) fail(EMG_ERR_STATE, "tiled pattern first needed inside a capture");
+  auto tp = std::make_unique<TiledPattern>();
+  const int umax = (int)((long)c.opt.tiled_smem_kb * 1024 / row_bytes);
+  const bool ok = build_tiled((int)h_rp.size() - 1, h_rp, h_ci, umax, 128, *tp, c.stream);
+  const TiledPattern *res = ok ? tp.get() : nullptr;
+  c.tiles[key] = ok ? std::move(tp) : nullptr;
+  return res;
+}
+
 // Geometry of the MT boundary values (assemble_rhs_mt, src/em_fwd.cc:488-580)
 // that does not depend on frequency or polarisation: per boundary edge its
 // midpoint depth, the blend weights of the four corner soundings and the
@@ -584,6 +604,8 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_block_inner_rtol") *value = o.block_inner_rtol;
   else if (k == "emg_block_inner_max_it") *value = o.block_inner_max_it;
   else if (k == "emg_block_fcg_mmax") *value = o.block_fcg_mmax;
+  else if (k == "emg_spmm_tiled") *value = o.spmm_tiled;
+  else if (k == "emg_tiled_smem_kb") *value = o.tiled_smem_kb;
   else fail(EMG_ERR_OPTION, "unknown option %s", key);
   EMG_API_END
 }
@@ -616,6 +638,7 @@ int emg_set_mesh(emg_context *c, int nv, const double *pts, int nt, const int *t
   c->h_non.assign(non, non + 4L * nt);
   c->h_ebdr.assign(ebdr, ebdr + ne);
   c->bnd_rank.release();
+  c->tiles.clear();
   c->pts.upload(c->h_pts, c->stream);
   c->tets.upload(c->h_tets, c->stream);
   c->attr.upload(c->h_attr, c->stream);
@@ -667,6 +690,7 @@ int emg_create_linear_system(emg_context *c, int tidx) {
   need(c && c->nt > 0, EMG_ERR_STATE, "create_linear_system before emg_set_mesh");
   EMG_CUDA(cudaSetDevice(c->device));
   c->tidx = tidx;
+  c->tiles.clear();
   build_sparsity(*c);
   build_vertex_pattern(*c);
   build_slot_maps(*c);
@@ -1236,7 +1260,9 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     if (pf.enabled)
       pf.begin("spmm_edge_fp64", c.stream, spmm_algo_bytes(n, c.nnz, K2, 8, true, SPMM_AX), &ev);
     if (pf.phases) pf.begin("phase_opB", c.stream, 0, &ph);
-    spmm_nnz<double>(K2, a, c.nnz, c.stream);
+    const TiledPattern *tp = tiled_pattern(c, c.rp.p, c.h_rp, c.h_ci, K2 * 8);
+    if (tp) spmm_tiled<double>(K2, a, *tp, c.stream);
+    else spmm_nnz<double>(K2, a, c.nnz, c.stream);
     if (pf.enabled) pf.end("spmm_edge_fp64", c.stream, ev);
     if (pf.phases) pf.end("phase_opB", c.stream, ph);
   };

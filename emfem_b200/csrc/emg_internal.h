@@ -125,6 +125,15 @@ struct DCsr {
   DBuf<T> l1c, l1m;  // l1 row sums of |vc| and |vm| (smoother diagonals)
 };
 
+// Row tiles of a CSR pattern with per-tile column lists (spmm_tiled): tile t
+// covers rows [t R, t R + R), its distinct columns are ucol[urp[t] ..
+// urp[t+1]), and lci[k] is nonzero k's index in that list.
+struct TiledPattern {
+  int n = 0, R = 0, ntiles = 0, umax = 0;
+  DBuf<int> urp, ucol;
+  DBuf<unsigned short> lci;
+};
+
 // ---------------------------------------------------------------------------
 // options (process_options, em_ctx.cc:100-175) + A_/B_ subset + emg keys
 // ---------------------------------------------------------------------------
@@ -167,6 +176,8 @@ struct Options {
   double block_inner_rtol = 1e-2;
   int block_inner_max_it = 30;
   int block_fcg_mmax = 2;
+  int spmm_tiled = 1;         // edge-column SpMMs gather through per-tile shared memory
+  int tiled_smem_kb = 64;     // shared memory budget of one tile
   int verbose = 0;
 };
 
@@ -228,10 +239,18 @@ struct Context {
   std::vector<int> h_bnd_rank;
   DBuf<int> bnd_rank;
   int n_bnd = 0;
+  // tiled copies of the fixed patterns, keyed by (row pointer, bytes per x row)
+  std::map<std::pair<const int *, int>, std::unique_ptr<TiledPattern>> tiles;
   std::unique_ptr<Workspace> ws;
   Context();
   ~Context();
 };
+
+// the tiled copy of a fixed pattern of the context for x rows of row_bytes
+// bytes (built on first use, before any capture); nullptr when tiling is off
+// or no tile size fits the shared-memory budget
+const TiledPattern *tiled_pattern(Context &c, const int *rp_dev, const std::vector<int> &h_rp,
+                                  const std::vector<int> &h_ci, int row_bytes);
 
 // records the message returned by emg_last_error() on this thread
 void set_last_error(const char *msg);

@@ -147,6 +147,60 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
   EMG_LAUNCH_CHECK();
 }
 
+// ---------------------------------------------------------------------------
+// tiled SpMM: per-tile column lists, x rows staged in shared memory
+// ---------------------------------------------------------------------------
+bool build_tiled(int n, const std::vector<int> &rp, const std::vector<int> &ci, int umax_limit, int r_max,
+                 TiledPattern &tp, cudaStream_t s) {
+  int R = 0, umax = 0;
+  std::vector<int> urp, ucol;
+  std::vector<unsigned short> lci;
+  if (!tile_rows(n, rp, ci, umax_limit, r_max, R, umax, urp, ucol, lci)) return false;
+  tp.n = n;
+  tp.R = R;
+  tp.ntiles = (int)urp.size() - 1;
+  tp.umax = umax;
+  tp.urp.upload(urp, s);
+  tp.ucol.upload(ucol, s);
+  tp.lci.upload(lci, s);
+  EMG_CUDA(cudaStreamSynchronize(s));  // host arrays go out of scope
+  return true;
+}
+
+template <typename T, int K, int V>
+static void tiled_launch(const SpmmArgs &a, const TiledPattern &tp, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    EMG_CUDA(cudaFuncSetAttribute(spmm_tiled_kernel<T, K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024));
+    attr = true;
+  }
+  const size_t smem = (size_t)tp.umax * K * sizeof(T);
+  if (smem > 227 * 1024) fail(EMG_ERR_ARG, "tile needs %zu bytes of shared memory", smem);
+  spmm_tiled_kernel<T, K, V><<<tp.ntiles, 256, smem, s>>>(a, TiledArgs{tp.R, tp.urp.p, tp.ucol.p, tp.lci.p});
+}
+
+template <typename T>
+void spmm_tiled(int K, const SpmmArgs &a, const TiledPattern &tp, cudaStream_t s) {
+  if (a.n <= 0) return;
+  if (a.n != tp.n) fail(EMG_ERR_STATE, "tiled pattern has %d rows, operator %d", tp.n, a.n);
+  constexpr int V0 = (int)(16 / sizeof(T));
+  switch (K) {
+  case 1: tiled_launch<T, 1, 1>(a, tp, s); break;
+  case 2: tiled_launch<T, 2, (V0 < 2 ? V0 : 2)>(a, tp, s); break;
+  case 4: tiled_launch<T, 4, (V0 < 4 ? V0 : 4)>(a, tp, s); break;
+  case 8: tiled_launch<T, 8, V0>(a, tp, s); break;
+  case 16: tiled_launch<T, 16, V0>(a, tp, s); break;
+  case 32: tiled_launch<T, 32, V0>(a, tp, s); break;
+  case 64: tiled_launch<T, 64, V0>(a, tp, s); break;
+  default: fail(EMG_ERR_ARG, "unsupported block width K=%d", K);
+  }
+  EMG_LAUNCH_CHECK();
+}
+
+template void spmm_tiled<float>(int, const SpmmArgs &, const TiledPattern &, cudaStream_t);
+template void spmm_tiled<double>(int, const SpmmArgs &, const TiledPattern &, cudaStream_t);
+
 template void spmm_nnz<float>(int, const SpmmArgs &, long, cudaStream_t);
 template void spmm_nnz<double>(int, const SpmmArgs &, long, cudaStream_t);
 

@@ -98,69 +98,14 @@ struct FusedOp {
   SpmmArgs a;
 };
 
-template <typename T, int K, int V, int NL>
-__global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
-  constexpr int CL = K / V;
-  constexpr int G = NL * CL;
-  static_assert(G <= 32 && (32 % G) == 0, "bad lane layout");
-  const int lane = threadIdx.x & 31;
-  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int row = gwarp * (32 / G) + lane / G;
-  const int sub = lane % G;
-  const int cb = sub % CL;      // column block
-  const int sl = sub / CL;      // nonzero slice
-  const T *__restrict__ vc = static_cast<const T *>(a.vc);
-  const T *__restrict__ vm = static_cast<const T *>(a.vm);
-  const T *__restrict__ x = static_cast<const T *>(a.x);
-  T acc[V];
-#pragma unroll
-  for (int i = 0; i < V; ++i) acc[i] = T(0);
-  T w[V];
-  const bool two = vm != nullptr;
-  if (two) {
-#pragma unroll
-    for (int i = 0; i < V; ++i) w[i] = (T)__ldg(a.omega + cb * V + i);
-  }
-  const bool valid = row < a.n;
-  if (valid) {
-    const int kb = __ldg(a.rp + row), ke = __ldg(a.rp + row + 1);
-    // U nonzeros per lane per round: all index/value loads of the round are
-    // issued before the dependent x gathers, so U gathers are in flight at
-    // once (rows are short, ~16 nonzeros, and split NL ways)
-    constexpr int U = 4;
-    for (int k0 = kb + sl; k0 < ke; k0 += NL * U) {
-      int j[U];
-      T c[U], m[U];
-      bool ok[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int k = k0 + u * NL;
-        ok[u] = k < ke;
-        j[u] = ok[u] ? __ldg(a.ci + k) : 0;
-        c[u] = ok[u] ? __ldg(vc + k) : T(0);
-        m[u] = (ok[u] && two) ? __ldg(vm + k) : T(0);
-      }
-      T xv[U][V];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (ok[u]) ldv<T, V>(x + (long)j[u] * K + cb * V, xv[u]);
-        else {
-#pragma unroll
-          for (int i = 0; i < V; ++i) xv[u][i] = T(0);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-#pragma unroll
-        for (int i = 0; i < V; ++i) acc[i] = fma(two ? c[u] + w[i] * m[u] : c[u], xv[u][i], acc[i]);
-    }
-  }
-#pragma unroll
-  for (int off = CL; off < G; off <<= 1)
-#pragma unroll
-    for (int i = 0; i < V; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
-  if (!valid || sl != 0) return;
+// Row epilogue shared by the SpMM kernels: combines the row product acc
+// (columns cb*V .. cb*V+V-1 of row `row`) with the vectors the mode needs and
+// stores the result row.
+template <typename T, int K, int V>
+__device__ __forceinline__ void spmm_epilogue(const SpmmArgs &a, int row, int cb, const T (&acc)[V], const T (&w)[V],
+                                              bool two) {
   const long o = (long)row * K + cb * V;
+  const T *__restrict__ x = static_cast<const T *>(a.x);
   T *y = static_cast<T *>(a.y);
   T out[V];
   switch (a.mode) {
@@ -227,6 +172,139 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
   }
   }
   stv<T, V>(y + o, out);
+}
+
+template <typename T, int K, int V, int NL>
+__global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
+  constexpr int CL = K / V;
+  constexpr int G = NL * CL;
+  static_assert(G <= 32 && (32 % G) == 0, "bad lane layout");
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int row = gwarp * (32 / G) + lane / G;
+  const int sub = lane % G;
+  const int cb = sub % CL;      // column block
+  const int sl = sub / CL;      // nonzero slice
+  const T *__restrict__ vc = static_cast<const T *>(a.vc);
+  const T *__restrict__ vm = static_cast<const T *>(a.vm);
+  const T *__restrict__ x = static_cast<const T *>(a.x);
+  T acc[V];
+#pragma unroll
+  for (int i = 0; i < V; ++i) acc[i] = T(0);
+  T w[V];
+  const bool two = vm != nullptr;
+#pragma unroll
+  for (int i = 0; i < V; ++i) w[i] = two ? (T)__ldg(a.omega + cb * V + i) : T(0);
+  const bool valid = row < a.n;
+  if (valid) {
+    const int kb = __ldg(a.rp + row), ke = __ldg(a.rp + row + 1);
+    // U nonzeros per lane per round: all index/value loads of the round are
+    // issued before the dependent x gathers, so U gathers are in flight at
+    // once (rows are short, ~16 nonzeros, and split NL ways)
+    constexpr int U = 4;
+    for (int k0 = kb + sl; k0 < ke; k0 += NL * U) {
+      int j[U];
+      T c[U], m[U];
+      bool ok[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * NL;
+        ok[u] = k < ke;
+        j[u] = ok[u] ? __ldg(a.ci + k) : 0;
+        c[u] = ok[u] ? __ldg(vc + k) : T(0);
+        m[u] = (ok[u] && two) ? __ldg(vm + k) : T(0);
+      }
+      T xv[U][V];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (ok[u]) ldv<T, V>(x + (long)j[u] * K + cb * V, xv[u]);
+        else {
+#pragma unroll
+          for (int i = 0; i < V; ++i) xv[u][i] = T(0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int i = 0; i < V; ++i) acc[i] = fma(two ? c[u] + w[i] * m[u] : c[u], xv[u][i], acc[i]);
+    }
+  }
+#pragma unroll
+  for (int off = CL; off < G; off <<= 1)
+#pragma unroll
+    for (int i = 0; i < V; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+  if (!valid || sl != 0) return;
+  spmm_epilogue<T, K, V>(a, row, cb, acc, w, two);
+}
+
+// Row tiles with their own column lists: tile t covers rows [t R, t R + R);
+// its distinct columns are ucol[urp[t] .. urp[t+1]) (ascending), and lci[k]
+// is nonzero k's position in that list.  One CTA stages the x rows of its
+// tile's columns in shared memory once, then every row gathers from there:
+// the L2 traffic of the gathers drops from nnz x K to (distinct columns) x K
+// values per tile.
+struct TiledArgs {
+  int R;
+  const int *urp, *ucol;
+  const unsigned short *lci;
+};
+
+template <typename T, int K, int V>
+__global__ void __launch_bounds__(256) spmm_tiled_kernel(SpmmArgs a, TiledArgs t) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *xs = reinterpret_cast<T *>(smem_raw);
+  typedef typename VecT<T, V>::type VT;
+  constexpr int CL = K / V;     // lanes over the columns of one row
+  constexpr int RPW = 32 / CL;  // rows per warp
+  static_assert(CL <= 32 && (32 % CL) == 0, "bad tiled lane layout");
+  const int tile = blockIdx.x;
+  const int u0 = __ldg(t.urp + tile), nu = __ldg(t.urp + tile + 1) - u0;
+  const T *__restrict__ x = static_cast<const T *>(a.x);
+  for (int idx = threadIdx.x; idx < nu * CL; idx += blockDim.x) {
+    const int u = idx / CL, cb = idx - u * CL;
+    const long g = __ldg(t.ucol + u0 + u);
+    *reinterpret_cast<VT *>(xs + u * K + cb * V) = __ldg(reinterpret_cast<const VT *>(x + g * K + cb * V));
+  }
+  __syncthreads();
+  const T *__restrict__ vc = static_cast<const T *>(a.vc);
+  const T *__restrict__ vm = static_cast<const T *>(a.vm);
+  const bool two = vm != nullptr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cb = lane % CL, sub = lane / CL;
+  T w[V];
+#pragma unroll
+  for (int i = 0; i < V; ++i) w[i] = two ? (T)__ldg(a.omega + cb * V + i) : T(0);
+  const int r0 = tile * t.R;
+  const int r1 = min(a.n, r0 + t.R);
+  const int nwarps = blockDim.x >> 5;
+  for (int row = r0 + warp * RPW + sub; row < r1; row += nwarps * RPW) {
+    T acc[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) acc[i] = T(0);
+    const int kb = __ldg(a.rp + row), ke = __ldg(a.rp + row + 1);
+    constexpr int U = 4;
+    for (int k0 = kb; k0 < ke; k0 += U) {
+      int j[U];
+      T c[U], m[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u;
+        const bool ok = k < ke;
+        j[u] = ok ? (int)__ldg(t.lci + k) : 0;
+        c[u] = ok ? __ldg(vc + k) : T(0);
+        m[u] = (ok && two) ? __ldg(vm + k) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (k0 + u >= ke) break;
+        const VT xv = *reinterpret_cast<const VT *>(xs + j[u] * K + cb * V);
+        const T *xe = reinterpret_cast<const T *>(&xv);
+#pragma unroll
+        for (int i = 0; i < V; ++i) acc[i] = fma(two ? c[u] + w[i] * m[u] : c[u], xe[i], acc[i]);
+      }
+    }
+    spmm_epilogue<T, K, V>(a, row, cb, acc, w, two);
+  }
 }
 
 }  // namespace emg

@@ -9,6 +9,7 @@
 
 #include "emg_internal.h"
 #include "emg_linalg.cuh"
+#include "emg_tiles.h"
 
 namespace emg {
 
@@ -31,6 +32,15 @@ double spmm_algo_bytes(long n, long nnz, int K, int elem, bool two_parts, int mo
 // nnz of the operator selects the row-length class of the tuning table
 template <typename T>
 void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s);
+
+// Tiles rows of a host CSR pattern for spmm_tiled: the largest R (a power of
+// two <= r_max, >= 8) whose busiest tile has at most umax_limit distinct
+// columns.  Returns false (tp untouched) when no such R exists.
+bool build_tiled(int n, const std::vector<int> &rp, const std::vector<int> &ci, int umax_limit, int r_max,
+                 TiledPattern &tp, cudaStream_t s);
+// SpMM through a tiled pattern (a.rp is the pattern's row pointer; a.ci unused)
+template <typename T>
+void spmm_tiled(int K, const SpmmArgs &a, const TiledPattern &tp, cudaStream_t s);
 
 // out[c] (+)= sum_i a[i*K+c] * b[i*K+c]   (FP64 accumulation); out must be zeroed
 template <typename T>

@@ -137,6 +137,7 @@ template <typename T>
 void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_ref) {
   cudaStream_t s = c.stream;
   StageClock clk(c);
+  ams.ctx = &c;
   ams.ne = c.ne;
   ams.nv = c.nv;
   ams.edges = c.edges.p;
@@ -385,12 +386,24 @@ void Ams<T>::spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s) {
   cudaEvent_t ev = nullptr;
   const char *bin = sizeof(T) == 4 ? "spmm_edge_fp32" : "spmm_edge_fp64";
   if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(ne, nnzB, K, sizeof(T), two, mode), &ev);
-  spmm_nnz<T>(K, a, nnzB, s);
+  const TiledPattern *tp = edge_tiles();
+  if (tp) spmm_tiled<T>(K, a, *tp, s);
+  else spmm_nnz<T>(K, a, nnzB, s);
   if (pf.enabled) pf.end(bin, s, ev);
 }
 
 template <typename T>
-void Ams<T>::emit_spmm(const SpmmArgs &a, long nnz, const char *bin, cudaStream_t s) {
+const TiledPattern *Ams<T>::edge_tiles() {
+  return ctx ? tiled_pattern(*ctx, brp, ctx->h_rp, ctx->h_ci, K * (int)sizeof(T)) : nullptr;
+}
+
+template <typename T>
+const TiledPattern *Ams<T>::gtb_tiles() {
+  return ctx ? tiled_pattern(*ctx, grp, ctx->h_grp, ctx->h_gci, K * (int)sizeof(T)) : nullptr;
+}
+
+template <typename T>
+void Ams<T>::emit_spmm(const SpmmArgs &a, long nnz, const char *bin, cudaStream_t s, const TiledPattern *tp) {
   if (rec) {
     FusedOp op;
     std::memset(&op, 0, sizeof(op));
@@ -403,7 +416,8 @@ void Ams<T>::emit_spmm(const SpmmArgs &a, long nnz, const char *bin, cudaStream_
   KernelProfiler &pf = profiler();
   cudaEvent_t ev = nullptr;
   if (pf.enabled) pf.begin(bin, s, spmm_algo_bytes(a.n, nnz, K, sizeof(T), a.vm != nullptr, a.mode), &ev);
-  spmm_nnz<T>(K, a, nnz, s);
+  if (tp) spmm_tiled<T>(K, a, *tp, s);
+  else spmm_nnz<T>(K, a, nnz, s);
   if (pf.enabled) pf.end(bin, s, ev);
 }
 
@@ -508,7 +522,7 @@ T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b,
     a.d = d;
     a.c1 = c1;
     a.c2 = c2;
-    emit_spmm(a, nnz, bin, s);
+    emit_spmm(a, nnz, bin, s, edge ? edge_tiles() : nullptr);
   };
   if (!cheb) {
     if (zero_guess) {
@@ -739,7 +753,9 @@ void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
         a.mode = SPMM_RES;
         a.r = a.d = nullptr;
         a.c1 = a.c2 = 0;
-        spmm_nnz<T>(K, a, nnzG, s);
+        const TiledPattern *tp = gtb_tiles();
+        if (tp) spmm_tiled<T>(K, a, *tp, s);
+        else spmm_nnz<T>(K, a, nnzG, s);
       }
     } else {
       if (zero) {

@@ -101,6 +101,7 @@ struct Ams {
     DBuf<double> cinv;           // n_distinct_omega x nc x nc
     std::vector<double> cinv_w;  // omegas the inverses were built for
   };
+  Context *ctx = nullptr;          // owner of the fixed patterns (tiled copies)
   DCsr<T> B;                       // values only: pattern is the context's
   const int *brp = nullptr, *bci = nullptr;
   long nnzB = 0;
@@ -162,7 +163,10 @@ struct Ams {
   // fails (and resets the barrier) when a fused launch reported a timeout
   void check_fused(cudaStream_t s);
   // step emitters: launch now, or append to *rec
-  void emit_spmm(const SpmmArgs &a, long nnz, const char *bin, cudaStream_t s);
+  void emit_spmm(const SpmmArgs &a, long nnz, const char *bin, cudaStream_t s, const TiledPattern *tp = nullptr);
+  // tiled copies of the edge pattern and of G^T B for this precision and K
+  const TiledPattern *edge_tiles();
+  const TiledPattern *gtb_tiles();
   void emit_jac0(int n, const T *b, const T *l1c, const T *l1m, double w, T *y, T *d, cudaStream_t s);
   void emit_coarse(int sp, const T *b, T *x, cudaStream_t s);
   // one smoothing application on operator A (edge B when A == nullptr);
