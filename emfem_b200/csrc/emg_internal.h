@@ -176,7 +176,7 @@ struct Options {
   double block_inner_rtol = 1e-2;
   int block_inner_max_it = 30;
   int block_fcg_mmax = 2;
-  int spmm_tiled = 1;         // edge-column SpMMs gather through per-tile shared memory
+  int spmm_tiled = 0;         // edge-column SpMMs gather through per-tile shared memory
   int tiled_smem_kb = 64;     // shared memory budget of one tile
   int verbose = 0;
 };

@@ -21,8 +21,9 @@ with the inner iteration cap of the reference: every variant converges to
 rtol 1e-10 and agrees with the exact discrete solution (sparse direct solve)
 to 1e-6 of its largest entry.
 
-3. The same bar with the edge-column SpMMs untiled (every x row gathered from
-L2) and with small tiles (16 KB of shared memory: more, shorter tiles).
+3. The same bar with the edge-column SpMMs tiled (x rows of each row tile
+staged once in shared memory), with the default 64 KB and with small tiles
+(16 KB: more, shorter tiles).
 """
 
 import numpy as np
@@ -88,8 +89,8 @@ def _direct(rp, ci, Cv, Mv, sr, si):
 @pytest.mark.parametrize("extra", ["-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 1 -emg_pi_coupled 1",
                                    "-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 3 -emg_pi_coupled 0",
                                    "-emg_fp32_cycle 034501 -emg_block_inner_max_it 100",
-                                   "-emg_spmm_tiled 0",
-                                   "-emg_tiled_smem_kb 16",
+                                   "-emg_spmm_tiled 1",
+                                   "-emg_spmm_tiled 1 -emg_tiled_smem_kb 16",
                                    "-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 7 -emg_fused_vcycle 1 "
                                    "-emg_fused_rows 400"])
 def test_pi_vector_space_cycles(mt_small, extra):
