@@ -167,6 +167,36 @@ def refine_fixed_number(err, fraction, flag=None):
     return flag
 
 
+# observation types (ObsType, src/em_defs.h:50-73)
+F_EX_RI, F_EY_RI, F_EZ_RI, F_HX_RI, F_HY_RI, F_HZ_RI = 111, 121, 131, 141, 151, 161
+F_EX_AP, F_EY_AP, F_EZ_AP, F_HX_AP, F_HY_AP, F_HZ_AP = 112, 122, 132, 142, 152, 162
+R_XY_AP, R_YX_AP = 212, 222
+Z_XX_RI, Z_XY_RI, Z_YX_RI, Z_YY_RI, T_ZX_RI, T_ZY_RI = 311, 321, 331, 341, 351, 361
+
+
+def calculate_response_mt(freq, fields, otype, ridx):
+    """calculate_response_mt (src/em_fwd.cc:747-800).  fields: (nrx, 4, 3)
+    complex -- E_xy, H_xy, E_yx, H_yx per receiver; returns one complex value
+    per observation (R_XY_AP / R_YX_AP: rho_a + 1j * phase in degrees)."""
+    f = np.ascontiguousarray(np.asarray(fields, dtype=np.complex128).reshape(-1, 4, 3))
+    ot, ri = _i32(otype), _i32(ridx)
+    out = np.zeros(ot.size, dtype=np.complex128)
+    _check(lib().emg_calculate_response_mt(C.c_double(freq), f.shape[0], _ptr(f.view(np.float64)), ot.size,
+                                           _ptr(ot), _ptr(ri), _ptr(out.view(np.float64))))
+    return out
+
+
+def calculate_response_csem(fields, otype, ridx):
+    """calculate_response_csem (src/em_fwd.cc:802-871).  fields: (nrx, 2, 3)
+    complex -- E, H per receiver."""
+    f = np.ascontiguousarray(np.asarray(fields, dtype=np.complex128).reshape(-1, 2, 3))
+    ot, ri = _i32(otype), _i32(ridx)
+    out = np.zeros(ot.size, dtype=np.complex128)
+    _check(lib().emg_calculate_response_csem(f.shape[0], _ptr(f.view(np.float64)), ot.size, _ptr(ot), _ptr(ri),
+                                             _ptr(out.view(np.float64))))
+    return out
+
+
 class EMContext:
     """Device-resident counterpart of the reference's EMContext (src/em_ctx.h:15-64).
 

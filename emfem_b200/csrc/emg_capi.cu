@@ -1101,6 +1101,79 @@ int emg_estimate_error(emg_context *c, int fidx, int tidx, double *err, double *
 }
 
 // refine_fixed_fraction (src/em_fwd.cc:1182-1215)
+// calculate_response_mt (em_fwd.cc:747-800): the reference's tensor
+// impedance and tipper formulas per observation, plus apparent resistivity
+// and phase from Z_XY / Z_YX.
+int emg_calculate_response_mt(double freq, int nrx, const double *fields, int nobs, const int *otype,
+                              const int *ridx, double *rsp) {
+  EMG_API_BEGIN
+  typedef std::complex<double> zc;
+  need(nobs >= 0 && nrx >= 0, EMG_ERR_ARG, "negative count");
+  need(nobs == 0 || (fields && otype && ridx && rsp), EMG_ERR_ARG, "null argument");
+  need(freq > 0, EMG_ERR_ARG, "frequency must be positive");
+  for (int o = 0; o < nobs; ++o) {
+    need(ridx[o] >= 0 && ridx[o] < nrx, EMG_ERR_ARG, "receiver index out of range");
+    const double *f = fields + 24 * (size_t)ridx[o];
+    auto at = [&](int block, int k) { return zc(f[6 * block + 2 * k], f[6 * block + 2 * k + 1]); };
+    const zc exy[3] = {at(0, 0), at(0, 1), at(0, 2)}, hxy[3] = {at(1, 0), at(1, 1), at(1, 2)};
+    const zc eyx[3] = {at(2, 0), at(2, 1), at(2, 2)}, hyx[3] = {at(3, 0), at(3, 1), at(3, 2)};
+    const zc den = hxy[0] * hyx[1] - hyx[0] * hxy[1];
+    zc v;
+    switch (otype[o]) {
+    case EMG_OBS_Z_XX_RI: v = (exy[0] * hyx[1] - eyx[0] * hxy[1]) / den; break;
+    case EMG_OBS_Z_XY_RI: v = (eyx[0] * hxy[0] - exy[0] * hyx[0]) / den; break;
+    case EMG_OBS_Z_YX_RI: v = (exy[1] * hyx[1] - eyx[1] * hxy[1]) / den; break;
+    case EMG_OBS_Z_YY_RI: v = (eyx[1] * hxy[0] - exy[1] * hyx[0]) / den; break;
+    case EMG_OBS_T_ZX_RI: v = (hxy[2] * hyx[1] - hyx[2] * hxy[1]) / den; break;
+    case EMG_OBS_T_ZY_RI: v = (hyx[2] * hxy[0] - hxy[2] * hyx[0]) / den; break;
+    case EMG_OBS_R_XY_AP:
+    case EMG_OBS_R_YX_AP: {
+      const zc z = otype[o] == EMG_OBS_R_XY_AP ? (eyx[0] * hxy[0] - exy[0] * hyx[0]) / den
+                                                : (exy[1] * hyx[1] - eyx[1] * hxy[1]) / den;
+      v = zc(std::norm(z) / (2.0 * PI * freq * MU), std::arg(std::conj(z)) / DTOR);
+      break;
+    }
+    default: fail(EMG_ERR_USER, "Data type %d not implemented.", otype[o]);
+    }
+    rsp[2 * (size_t)o] = v.real();
+    rsp[2 * (size_t)o + 1] = v.imag();
+  }
+  EMG_API_END
+}
+
+// calculate_response_csem (em_fwd.cc:802-871)
+int emg_calculate_response_csem(int nrx, const double *fields, int nobs, const int *otype, const int *ridx,
+                                double *rsp) {
+  EMG_API_BEGIN
+  typedef std::complex<double> zc;
+  need(nobs >= 0 && nrx >= 0, EMG_ERR_ARG, "negative count");
+  need(nobs == 0 || (fields && otype && ridx && rsp), EMG_ERR_ARG, "null argument");
+  for (int o = 0; o < nobs; ++o) {
+    need(ridx[o] >= 0 && ridx[o] < nrx, EMG_ERR_ARG, "receiver index out of range");
+    const double *f = fields + 12 * (size_t)ridx[o];
+    auto comp = [&](int k) { return zc(f[2 * k], f[2 * k + 1]); };
+    zc v;
+    switch (otype[o]) {
+    case EMG_OBS_F_EX_RI: v = comp(0); break;
+    case EMG_OBS_F_EY_RI: v = comp(1); break;
+    case EMG_OBS_F_EZ_RI: v = comp(2); break;
+    case EMG_OBS_F_HX_RI: v = comp(3); break;
+    case EMG_OBS_F_HY_RI: v = comp(4); break;
+    case EMG_OBS_F_HZ_RI: v = comp(5); break;
+    case EMG_OBS_F_EX_AP: v = std::log(comp(0)); break;
+    case EMG_OBS_F_EY_AP: v = std::log(comp(1)); break;
+    case EMG_OBS_F_EZ_AP: v = std::log(comp(2)); break;
+    case EMG_OBS_F_HX_AP: v = std::log(comp(3)); break;
+    case EMG_OBS_F_HY_AP: v = std::log(comp(4)); break;
+    case EMG_OBS_F_HZ_AP: v = std::log(comp(5)); break;
+    default: fail(EMG_ERR_USER, "Data type %d not implemented.", otype[o]);
+    }
+    rsp[2 * (size_t)o] = v.real();
+    rsp[2 * (size_t)o + 1] = v.imag();
+  }
+  EMG_API_END
+}
+
 int emg_refine_fixed_fraction(int n, const double *err, double fraction, unsigned char *flag) {
   EMG_API_BEGIN
   need(n >= 0 && (n == 0 || (err && flag)), EMG_ERR_ARG, "null argument");

@@ -167,6 +167,48 @@ int emg_refine_fixed_number(int n, const double *err, double fraction, unsigned 
 int emg_interpolate_fields(emg_context *ctx, int target, int fidx, int n, const double *pts,
                            const int *tets, double *eh);
 
+/* Observation types (ObsType, src/em_defs.h:50-73). */
+#define EMG_OBS_F_EX_RI 111
+#define EMG_OBS_F_EY_RI 121
+#define EMG_OBS_F_EZ_RI 131
+#define EMG_OBS_F_HX_RI 141
+#define EMG_OBS_F_HY_RI 151
+#define EMG_OBS_F_HZ_RI 161
+#define EMG_OBS_F_EX_AP 112
+#define EMG_OBS_F_EY_AP 122
+#define EMG_OBS_F_EZ_AP 132
+#define EMG_OBS_F_HX_AP 142
+#define EMG_OBS_F_HY_AP 152
+#define EMG_OBS_F_HZ_AP 162
+#define EMG_OBS_R_XY_AP 212
+#define EMG_OBS_R_YX_AP 222
+#define EMG_OBS_Z_XX_RI 311
+#define EMG_OBS_Z_XY_RI 321
+#define EMG_OBS_Z_YX_RI 331
+#define EMG_OBS_Z_YY_RI 341
+#define EMG_OBS_T_ZX_RI 351
+#define EMG_OBS_T_ZY_RI 361
+
+/* calculate_response_mt (src/em_fwd.cc:747-800) from the fields at the
+ * receivers.  fields: per receiver 12 complex values, interleaved re/im:
+ * E and H of the XY polarisation, then E and H of the YX polarisation (what
+ * emg_interpolate_fields returns for EMG_SOL_MT_XY and EMG_SOL_MT_YX).  For
+ * observation o: type otype[o], receiver ridx[o] -> rsp[2o], rsp[2o+1].
+ * Z_XX/XY/YX/YY_RI and T_ZX/ZY_RI as the reference.  R_XY_AP / R_YX_AP,
+ * which the reference declares but refuses, give the apparent resistivity
+ * |Z|^2 / (w mu) (real part) and the phase of conj(Z) in degrees (imaginary
+ * part: the e^{-iwt} phase of the reference's e^{+iwt} fields; a halfspace
+ * gives 45 and -135).  Other types: EMG_ERR_USER, as the reference.  Host
+ * only; needs no context. */
+int emg_calculate_response_mt(double freq, int nrx, const double *fields, int nobs, const int *otype,
+                              const int *ridx, double *rsp);
+
+/* calculate_response_csem (src/em_fwd.cc:802-871): fields per receiver are 6
+ * complex values (E, H); F_*_RI give the component, F_*_AP its complex
+ * logarithm.  Host only. */
+int emg_calculate_response_csem(int nrx, const double *fields, int nobs, const int *otype, const int *ridx,
+                                double *rsp);
+
 /* ---- batched fast path (no reference counterpart: replaces the per-task
  * loop of forward_mt/forward_csem, src/em_fwd.cc:1320-1439) -------------
  * Solves k right-hand sides with individual frequencies as one block:

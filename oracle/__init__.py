@@ -265,3 +265,22 @@ def interpolate_fields(mesh: Mesh, t, p, freq, er, ei):
     o = out.reshape(6, 2)
     z = o[:, 0] + 1j * o[:, 1]
     return z[:3], z[3:]
+
+
+def response_mt(freq, fields, otype):
+    """calculate_response_mt for one receiver; fields (4, 3) complex (E_xy, H_xy,
+    E_yx, H_yx).  Returns the complex value or None for a refused type."""
+    f = np.ascontiguousarray(np.asarray(fields, dtype=np.complex128).reshape(4, 3)).view(np.float64)
+    out = np.zeros(2)
+    lib().orc_response_mt.restype = C.c_int
+    rc = lib().orc_response_mt(C.c_double(freq), _p(f), C.c_int(otype), _p(out))
+    return None if rc != 0 else out[0] + 1j * out[1]
+
+
+def response_csem(fields, otype):
+    """calculate_response_csem for one receiver; fields (2, 3) complex (E, H)."""
+    f = np.ascontiguousarray(np.asarray(fields, dtype=np.complex128).reshape(2, 3)).view(np.float64)
+    out = np.zeros(2)
+    lib().orc_response_csem.restype = C.c_int
+    rc = lib().orc_response_csem(_p(f), C.c_int(otype), _p(out))
+    return None if rc != 0 else out[0] + 1j * out[1]

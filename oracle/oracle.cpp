@@ -1548,4 +1548,56 @@ void orc_interpolate_fields(const OrcMesh *m, int t, const double *p, double fre
   }
 }
 
+// calculate_response_mt (em_fwd.cc:747-800): tensor impedance and tipper
+// entries from the fields of the two polarisations at one receiver.
+// f: e_xy[3], h_xy[3], e_yx[3], h_yx[3] (complex, interleaved).  Types as
+// the reference's ObsType (em_defs.h:50-73); 212/222 (apparent resistivity
+// and phase, declared but refused by the reference) are derived from the
+// Z_XY / Z_YX entries: rho_a = |Z|^2 / (w mu) and the phase of conj(Z) in
+// degrees.  Returns 0, or -1 for a type the path does not compute.
+int orc_response_mt(double freq, const double *f, int otype, double *out) {
+  cplx e_xy[3], h_xy[3], e_yx[3], h_yx[3];
+  for (int k = 0; k < 3; ++k) {
+    e_xy[k] = cplx(f[2 * k], f[2 * k + 1]);
+    h_xy[k] = cplx(f[6 + 2 * k], f[6 + 2 * k + 1]);
+    e_yx[k] = cplx(f[12 + 2 * k], f[12 + 2 * k + 1]);
+    h_yx[k] = cplx(f[18 + 2 * k], f[18 + 2 * k + 1]);
+  }
+  const cplx det = h_xy[0] * h_yx[1] - h_yx[0] * h_xy[1];
+  cplx r;
+  switch (otype) {
+  case 311: r = (e_xy[0] * h_yx[1] - e_yx[0] * h_xy[1]) / det; break;
+  case 321: r = (e_yx[0] * h_xy[0] - e_xy[0] * h_yx[0]) / det; break;
+  case 331: r = (e_xy[1] * h_yx[1] - e_yx[1] * h_xy[1]) / det; break;
+  case 341: r = (e_yx[1] * h_xy[0] - e_xy[1] * h_yx[0]) / det; break;
+  case 351: r = (h_xy[2] * h_yx[1] - h_yx[2] * h_xy[1]) / det; break;
+  case 361: r = (h_yx[2] * h_xy[0] - h_xy[2] * h_yx[0]) / det; break;
+  case 212:
+  case 222: {
+    const cplx z = otype == 212 ? (e_yx[0] * h_xy[0] - e_xy[0] * h_yx[0]) / det
+                                : (e_xy[1] * h_yx[1] - e_yx[1] * h_xy[1]) / det;
+    const double w = 2.0 * PI * freq;
+    r = cplx(std::norm(z) / (w * MU), std::atan2(-z.imag(), z.real()) * 180.0 / PI);
+    break;
+  }
+  default: return -1;
+  }
+  out[0] = r.real();
+  out[1] = r.imag();
+  return 0;
+}
+
+// calculate_response_csem (em_fwd.cc:802-871): field components (RI) or
+// their complex logarithms (AP).  f: e[3], h[3] (complex, interleaved).
+int orc_response_csem(const double *f, int otype, double *out) {
+  const int comp = otype / 10 % 10;  // 1..6: Ex, Ey, Ez, Hx, Hy, Hz
+  const int kind = otype % 10;       // 1: RI, 2: AP
+  if (otype / 100 != 1 || comp < 1 || comp > 6 || (kind != 1 && kind != 2)) return -1;
+  cplx v(f[2 * (comp - 1)], f[2 * (comp - 1) + 1]);
+  if (kind == 2) v = std::log(v);
+  out[0] = v.real();
+  out[1] = v.imag();
+  return 0;
+}
+
 }  // extern "C"
