@@ -97,6 +97,12 @@ _SIGS = {
     "emg_assemble_rhs_mt_block": ([_P, _I, _P, _P, _P], _I),
     "emg_assemble_rhs_mt_block_dev": ([_P, _I, _P, _P, _P], _I),
     "emg_estimate_error_noalloc": ([_P, _I, _I, _P, _P], _I),
+    "emg_calculate_response_mt": ([_D, _I, _P, _I, _P, _P, _P], _I),
+    "emg_calculate_response_csem": ([_I, _P, _I, _P, _P, _P], _I),
+    "emg_point_index_create": ([_I, _P, _I, _P, _P], _P),
+    "emg_point_index_find": ([_P, _I, _P, _P], _I),
+    "emg_point_index_destroy": ([_P], None),
+    "emg_find_cell_around_point": ([_P, _I, _P, _P], _I),
 }
 
 
@@ -167,6 +173,35 @@ def refine_fixed_number(err, fraction, flag=None):
     return flag
 
 
+class PointIndex:
+    """find_cell_around_point (src/em_mesh.cc:527-566) over a mesh's
+    pointlist / tetrahedronlist / neighborlist, reusable across queries."""
+
+    def __init__(self, mesh):
+        self._arrs = (_f64(mesh.points), _i32(mesh.tets), _i32(mesh.neighbors))
+        self._h = lib().emg_point_index_create(mesh.n_vertices, _ptr(self._arrs[0]), mesh.n_tets,
+                                               _ptr(self._arrs[1]), _ptr(self._arrs[2]))
+        if not self._h:
+            raise EMGError(EMG_ERR_ARG, lib().emg_last_error().decode())
+
+    def find(self, pts):
+        p = _f64(np.asarray(pts).reshape(-1, 3))
+        out = np.zeros(p.shape[0], dtype=np.int32)
+        _check(lib().emg_point_index_find(self._h, p.shape[0], _ptr(p), _ptr(out)))
+        return out
+
+    def close(self):
+        if self._h:
+            lib().emg_point_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # observation types (ObsType, src/em_defs.h:50-73)
 F_EX_RI, F_EY_RI, F_EZ_RI, F_HX_RI, F_HY_RI, F_HZ_RI = 111, 121, 131, 141, 151, 161
 F_EX_AP, F_EY_AP, F_EZ_AP, F_HX_AP, F_HY_AP, F_HZ_AP = 112, 122, 132, 142, 152, 162
@@ -181,7 +216,7 @@ def calculate_response_mt(freq, fields, otype, ridx):
     f = np.ascontiguousarray(np.asarray(fields, dtype=np.complex128).reshape(-1, 4, 3))
     ot, ri = _i32(otype), _i32(ridx)
     out = np.zeros(ot.size, dtype=np.complex128)
-    _check(lib().emg_calculate_response_mt(C.c_double(freq), f.shape[0], _ptr(f.view(np.float64)), ot.size,
+    _check(lib().emg_calculate_response_mt(float(freq), f.shape[0], _ptr(f.view(np.float64)), ot.size,
                                            _ptr(ot), _ptr(ri), _ptr(out.view(np.float64))))
     return out
 
@@ -417,6 +452,13 @@ class EMContext:
         om = _f64(omegas)
         _check(lib().emg_spmv_complex_dev(self._h, om.size, _ptr(om), C.c_void_p(x_ptr), C.c_void_p(y_ptr),
                                           int(conj_out)))
+
+    def find_cell_around_point(self, pts):
+        """find_cell_around_point (src/em_mesh.cc:527-566) on the context's mesh."""
+        p = _f64(np.asarray(pts).reshape(-1, 3))
+        out = np.zeros(p.shape[0], dtype=np.int32)
+        _check(lib().emg_find_cell_around_point(self._h, p.shape[0], _ptr(p), _ptr(out)))
+        return out
 
     def last_kernel_ms(self, name):
         v = C.c_double()

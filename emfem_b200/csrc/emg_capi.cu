@@ -18,6 +18,7 @@
 #include "emg_internal.h"
 #include "emg_kernels.cuh"
 #include "emg_linalg.h"
+#include "emg_locate.h"
 #include "emg_solver.h"
 
 namespace emg {
@@ -639,6 +640,7 @@ int emg_set_mesh(emg_context *c, int nv, const double *pts, int nt, const int *t
   c->h_ebdr.assign(ebdr, ebdr + ne);
   c->bnd_rank.release();
   c->tiles.clear();
+  c->locator.reset();
   c->pts.upload(c->h_pts, c->stream);
   c->tets.upload(c->h_tets, c->stream);
   c->attr.upload(c->h_attr, c->stream);
@@ -1101,6 +1103,52 @@ int emg_estimate_error(emg_context *c, int fidx, int tidx, double *err, double *
 }
 
 // refine_fixed_fraction (src/em_fwd.cc:1182-1215)
+struct emg_point_index {
+  emg::PointIndex index;
+  emg_point_index(int nv, const double *pts, int nt, const int *tets, const int *nbr)
+      : index(nv, pts, nt, tets, nbr) {}
+};
+
+static void locate_all(const PointIndex &ix, int n, const double *pts, int *out) {
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < n; ++i) out[i] = ix.find(pts + 3 * (size_t)i);
+}
+
+emg_point_index *emg_point_index_create(int nv, const double *pts, int nt, const int *tets, const int *nbr) {
+  try {
+    need(nv > 0 && nt > 0 && pts && tets && nbr, EMG_ERR_ARG, "empty or null mesh");
+    for (long i = 0; i < 4L * nt; ++i) {
+      need(tets[i] >= 0 && tets[i] < nv, EMG_ERR_ARG, "tetrahedronlist index out of range");
+      need(nbr[i] >= -1 && nbr[i] < nt, EMG_ERR_ARG, "neighborlist index out of range");
+    }
+    return new emg_point_index(nv, pts, nt, tets, nbr);
+  } catch (const emg::Error &e) {
+    emg::g_last_error = e.what();
+  } catch (const std::exception &e) {
+    emg::g_last_error = e.what();
+  }
+  return nullptr;
+}
+
+int emg_point_index_find(const emg_point_index *idx, int n, const double *pts, int *tets_out) {
+  EMG_API_BEGIN
+  need(idx && n >= 0 && (n == 0 || (pts && tets_out)), EMG_ERR_ARG, "null argument");
+  locate_all(idx->index, n, pts, tets_out);
+  EMG_API_END
+}
+
+void emg_point_index_destroy(emg_point_index *idx) { delete idx; }
+
+int emg_find_cell_around_point(emg_context *c, int n, const double *pts, int *tets_out) {
+  EMG_API_BEGIN
+  need(c && n >= 0 && (n == 0 || (pts && tets_out)), EMG_ERR_ARG, "null argument");
+  need(c->nt > 0, EMG_ERR_STATE, "find_cell_around_point before emg_set_mesh");
+  if (!c->locator)
+    c->locator = std::make_shared<PointIndex>(c->nv, c->h_pts.data(), c->nt, c->h_tets.data(), c->h_nbr.data());
+  locate_all(*c->locator, n, pts, tets_out);
+  EMG_API_END
+}
+
 // calculate_response_mt (em_fwd.cc:747-800): the reference's tensor
 // impedance and tipper formulas per observation, plus apparent resistivity
 // and phase from Z_XY / Z_YX.

@@ -239,6 +239,8 @@ struct Context {
   std::vector<int> h_bnd_rank;
   DBuf<int> bnd_rank;
   int n_bnd = 0;
+  // point location index over the host mesh (built on first use)
+  std::shared_ptr<struct PointIndex> locator;
   // tiled copies of the fixed patterns, keyed by (row pointer, bytes per x row)
   std::map<std::pair<const int *, int>, std::unique_ptr<TiledPattern>> tiles;
   std::unique_ptr<Workspace> ws;

@@ -167,6 +167,21 @@ int emg_refine_fixed_number(int n, const double *err, double fraction, unsigned 
 int emg_interpolate_fields(emg_context *ctx, int target, int fidx, int n, const double *pts,
                            const int *tets, double *eh);
 
+/* find_cell_around_point (src/em_mesh.cc:527-566) for many points: the
+ * reference's walk (from the last tet of the closest vertex, breadth-first
+ * over neighbours, first tet whose four orientations are >= 0), with the
+ * closest vertex from a uniform grid and no per-query O(T) clearing.  The
+ * index copies the arrays (tetgenio layout: pointlist, tetrahedronlist,
+ * neighborlist with -1 on the boundary).  tets_out[i] = -1 where no tet
+ * contains the point (the reference asserts).  Host only. */
+typedef struct emg_point_index emg_point_index;
+emg_point_index *emg_point_index_create(int nv, const double *pts, int nt, const int *tets, const int *nbr);
+int emg_point_index_find(const emg_point_index *idx, int n, const double *pts, int *tets_out);
+void emg_point_index_destroy(emg_point_index *idx);
+/* the same on the context's mesh (index built on first use, dropped by the
+ * next emg_set_mesh) */
+int emg_find_cell_around_point(emg_context *ctx, int n, const double *pts, int *tets_out);
+
 /* Observation types (ObsType, src/em_defs.h:50-73). */
 #define EMG_OBS_F_EX_RI 111
 #define EMG_OBS_F_EY_RI 121

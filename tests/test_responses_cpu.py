@@ -76,3 +76,32 @@ def test_halfspace_apparent_resistivity_and_phase(rho, freq):
     assert abs(r[0].real - rho) <= 1e-9 * rho and abs(r[1].real - rho) <= 1e-9 * rho
     assert abs(r[0].imag - 45.0) <= 1e-9 and abs(r[1].imag + 135.0) <= 1e-9
     assert abs(r[2] - eh[0] / eh[1]) <= 1e-14 * abs(r[2])
+
+
+# ---------------------------------------------------------------------------
+# point location (find_cell_around_point, src/em_mesh.cc:527-566)
+# ---------------------------------------------------------------------------
+def test_point_location_matches_oracle_walk():
+    """The indexed walk returns the oracle's tet for every point: random
+    interior points, receivers on the surface (z = 0 lies on mesh faces, where
+    two tets contain the point and the walk order decides) and mesh vertices
+    (shared by many tets); points outside the mesh give -1."""
+    from emfem_b200 import meshgen as mg
+    prob = mg.mt_halfspace_block(4000, freqs=(1.0,), name="loc")
+    m = prob.mesh
+    om = O.Mesh(m)
+    rng = np.random.default_rng(11)
+    lo, hi = m.points.min(axis=0), m.points.max(axis=0)
+    inner = lo + (hi - lo) * rng.uniform(0.02, 0.98, (400, 3))
+    surf = np.column_stack([rng.uniform(lo[0] * 0.5, hi[0] * 0.5, 60), rng.uniform(lo[1] * 0.5, hi[1] * 0.5, 60),
+                            np.zeros(60)])
+    verts = m.points[rng.choice(m.n_vertices, 60, replace=False)]
+    pts = np.vstack([inner, surf, verts, prob.survey.rx])
+    ix = E.PointIndex(m)
+    got = ix.find(pts)
+    ref = O.find_cell(om, pts)
+    assert (ref >= 0).all()
+    assert np.array_equal(got, ref)
+    outside = np.array([[hi[0] * 2, 0.0, 0.0], [0.0, lo[1] * 3, 0.0]])
+    assert (ix.find(outside) == -1).all()
+    ix.close()
