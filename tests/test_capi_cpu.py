@@ -55,6 +55,33 @@ def test_options_parsing():
         assert c.get_option("refine_fraction") == 0.1
 
 
+def test_solver_extension_options():
+    """emg_* keys of the batched path and the AMS variants: defaults, round
+    trip, and rejection of out-of-range values."""
+    with E.EMContext(-1) as c:
+        defaults = {"emg_block_inner_max_it": 30, "emg_block_inner_rtol": 1e-2, "emg_block_fcg_mmax": 2,
+                    "emg_pi_coupled": 0, "emg_fused_vcycle": 0, "emg_spmm_tiled": 0, "emg_tiled_smem_kb": 64,
+                    "emg_graphs": 1, "emg_inner_precision": 0}
+        for k, v in defaults.items():
+            assert c.get_option(k) == v, k
+        c.process_options("-emg_block_inner_max_it 45 -emg_block_inner_rtol 0.05 -emg_block_fcg_mmax 3 "
+                          "-emg_pi_coupled 1 -emg_fused_vcycle -emg_fused_rows 5000 -emg_fused_blocks_per_sm 2 "
+                          "-emg_spmm_tiled 1 -emg_tiled_smem_kb 32 -B_pc_hypre_ams_cycle_type 7")
+        got = {k: c.get_option(k) for k in ("emg_block_inner_max_it", "emg_block_inner_rtol", "emg_block_fcg_mmax",
+                                            "emg_pi_coupled", "emg_fused_vcycle", "emg_fused_rows",
+                                            "emg_fused_blocks_per_sm", "emg_spmm_tiled", "emg_tiled_smem_kb")}
+        assert got == {"emg_block_inner_max_it": 45, "emg_block_inner_rtol": 0.05, "emg_block_fcg_mmax": 3,
+                       "emg_pi_coupled": 1, "emg_fused_vcycle": 1, "emg_fused_rows": 5000,
+                       "emg_fused_blocks_per_sm": 2, "emg_spmm_tiled": 1, "emg_tiled_smem_kb": 32}
+        for ct in (1, 3, 5, 7, 11, 13):
+            c.process_options("-B_pc_hypre_ams_cycle_type %d" % ct)
+        for bad in ("-emg_block_inner_max_it 0", "-emg_block_inner_rtol 0", "-emg_block_fcg_mmax 31",
+                    "-emg_tiled_smem_kb 300", "-B_pc_hypre_ams_cycle_type 14"):
+            with pytest.raises(E.EMGError) as ei:
+                c.process_options(bad)
+            assert ei.value.code == E.api.EMG_ERR_OPTION
+
+
 def test_host_only_context_refuses_device_work():
     with E.EMContext(-1) as c:
         from emfem_b200 import meshgen as mg
