@@ -212,7 +212,8 @@ Z_XX_RI, Z_XY_RI, Z_YX_RI, Z_YY_RI, T_ZX_RI, T_ZY_RI = 311, 321, 331, 341, 351, 
 def calculate_response_mt(freq, fields, otype, ridx):
     """calculate_response_mt (src/em_fwd.cc:747-800).  fields: (nrx, 4, 3)
     complex -- E_xy, H_xy, E_yx, H_yx per receiver; returns one complex value
-    per observation (R_XY_AP / R_YX_AP: rho_a + 1j * phase in degrees)."""
+    per observation (R_XY_AP / R_YX_AP: log(rho_a) + 1j * phase in radians,
+    the reference's AP pair)."""
     f = np.ascontiguousarray(np.asarray(fields, dtype=np.complex128).reshape(-1, 4, 3))
     ot, ri = _i32(otype), _i32(ridx)
     out = np.zeros(ot.size, dtype=np.complex128)

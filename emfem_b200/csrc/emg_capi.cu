@@ -1178,7 +1178,9 @@ int emg_calculate_response_mt(double freq, int nrx, const double *fields, int no
     case EMG_OBS_R_YX_AP: {
       const zc z = otype[o] == EMG_OBS_R_XY_AP ? (eyx[0] * hxy[0] - exy[0] * hyx[0]) / den
                                                 : (exy[1] * hyx[1] - eyx[1] * hxy[1]) / den;
-      v = zc(std::norm(z) / (2.0 * PI * freq * MU), std::arg(std::conj(z)) / DTOR);
+      // the reference's AP pair: log amplitude and phase in radians (as
+      // read_emd stores the observation and save_rsp writes it back)
+      v = zc(std::log(std::norm(z) / (2.0 * PI * freq * MU)), std::arg(std::conj(z)));
       break;
     }
     default: fail(EMG_ERR_USER, "Data type %d not implemented.", otype[o]);

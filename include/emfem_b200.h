@@ -210,11 +210,12 @@ int emg_find_cell_around_point(emg_context *ctx, int n, const double *pts, int *
  * emg_interpolate_fields returns for EMG_SOL_MT_XY and EMG_SOL_MT_YX).  For
  * observation o: type otype[o], receiver ridx[o] -> rsp[2o], rsp[2o+1].
  * Z_XX/XY/YX/YY_RI and T_ZX/ZY_RI as the reference.  R_XY_AP / R_YX_AP,
- * which the reference declares but refuses, give the apparent resistivity
- * |Z|^2 / (w mu) (real part) and the phase of conj(Z) in degrees (imaginary
- * part: the e^{-iwt} phase of the reference's e^{+iwt} fields; a halfspace
- * gives 45 and -135).  Other types: EMG_ERR_USER, as the reference.  Host
- * only; needs no context. */
+ * which the reference declares but refuses, give the reference's AP pair
+ * (read_emd / save_rsp, src/em_io.cc:248-262, 360-372): the log of the
+ * apparent resistivity |Z|^2 / (w mu) (real part) and the phase of conj(Z)
+ * in radians (imaginary part: the e^{-iwt} phase of the reference's e^{+iwt}
+ * fields; a halfspace gives pi/4 and -3pi/4).  Other types: EMG_ERR_USER, as
+ * the reference.  Host only; needs no context. */
 int emg_calculate_response_mt(double freq, int nrx, const double *fields, int nobs, const int *otype,
                               const int *ridx, double *rsp);
 

@@ -1553,8 +1553,9 @@ void orc_interpolate_fields(const OrcMesh *m, int t, const double *p, double fre
 // f: e_xy[3], h_xy[3], e_yx[3], h_yx[3] (complex, interleaved).  Types as
 // the reference's ObsType (em_defs.h:50-73); 212/222 (apparent resistivity
 // and phase, declared but refused by the reference) are derived from the
-// Z_XY / Z_YX entries: rho_a = |Z|^2 / (w mu) and the phase of conj(Z) in
-// degrees.  Returns 0, or -1 for a type the path does not compute.
+// Z_XY / Z_YX entries as the reference's AP pair (em_io.cc:248-262): log of
+// rho_a = |Z|^2 / (w mu) and the phase of conj(Z) in radians.  Returns 0,
+// or -1 for a type the path does not compute.
 int orc_response_mt(double freq, const double *f, int otype, double *out) {
   cplx e_xy[3], h_xy[3], e_yx[3], h_yx[3];
   for (int k = 0; k < 3; ++k) {
@@ -1577,7 +1578,7 @@ int orc_response_mt(double freq, const double *f, int otype, double *out) {
     const cplx z = otype == 212 ? (e_yx[0] * h_xy[0] - e_xy[0] * h_yx[0]) / det
                                 : (e_xy[1] * h_yx[1] - e_yx[1] * h_xy[1]) / det;
     const double w = 2.0 * PI * freq;
-    r = cplx(std::norm(z) / (w * MU), std::atan2(-z.imag(), z.real()) * 180.0 / PI);
+    r = cplx(std::log(std::norm(z) / (w * MU)), std::atan2(-z.imag(), z.real()));
     break;
   }
   default: return -1;

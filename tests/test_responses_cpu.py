@@ -5,8 +5,9 @@ and apparent resistivity / phase against the exact layered-earth plane wave.
 Tolerances: the response formulas are a handful of complex products and one
 division; library and oracle evaluate the same expressions in the same order,
 so they agree to 1e-14 relative.  Against the analytic 1-D solution the
-derived rho_a and phase agree to 1e-9 relative / 1e-9 degrees (the plane-wave
-fields carry no discretisation error).
+derived rho_a and phase (the reference's AP pair: log amplitude, radians)
+agree to 1e-9 relative / 1e-9 degrees (the plane-wave fields carry no
+discretisation error).
 """
 
 import numpy as np
@@ -73,8 +74,9 @@ def test_halfspace_apparent_resistivity_and_phase(rho, freq):
     f = np.zeros((1, 4, 3), dtype=np.complex128)
     f[0, 0, 0], f[0, 1, 1], f[0, 2, 1], f[0, 3, 0] = eh[0], eh[1], eh[2], eh[3]
     r = E.calculate_response_mt(freq, f, [E.api.R_XY_AP, E.api.R_YX_AP, E.api.Z_XY_RI], [0, 0, 0])
-    assert abs(r[0].real - rho) <= 1e-9 * rho and abs(r[1].real - rho) <= 1e-9 * rho
-    assert abs(r[0].imag - 45.0) <= 1e-9 and abs(r[1].imag + 135.0) <= 1e-9
+    # the reference's AP pair: log(rho_a) and the phase in radians
+    assert abs(np.exp(r[0].real) - rho) <= 1e-9 * rho and abs(np.exp(r[1].real) - rho) <= 1e-9 * rho
+    assert abs(np.degrees(r[0].imag) - 45.0) <= 1e-9 and abs(np.degrees(r[1].imag) + 135.0) <= 1e-9
     assert abs(r[2] - eh[0] / eh[1]) <= 1e-14 * abs(r[2])
 
 
