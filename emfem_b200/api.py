@@ -103,6 +103,11 @@ _SIGS = {
     "emg_point_index_find": ([_P, _I, _P, _P], _I),
     "emg_point_index_destroy": ([_P], None),
     "emg_find_cell_around_point": ([_P, _I, _P, _P], _I),
+    "emg_survey_read_emd": ([C.c_char_p], _P),
+    "emg_survey_sizes": ([_P, _P, _P, _P, _P], _I),
+    "emg_survey_get": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
+    "emg_survey_write_rsp": ([_P, C.c_char_p, _P], _I),
+    "emg_survey_destroy": ([_P], None),
 }
 
 
@@ -193,6 +198,47 @@ class PointIndex:
     def close(self):
         if self._h:
             lib().emg_point_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Survey:
+    """A survey file in the reference's .emd layout (read_emd,
+    src/em_io.cc:202-287): freqs, tx (n, 7), rx (n, 3) and the observations
+    (otype, fidx, tidx, ridx, obs, obserr; AP types as log amplitude and
+    phase in radians).  write_rsp writes save_rsp's layout."""
+
+    def __init__(self, path):
+        self._h = lib().emg_survey_read_emd(os.fsencode(path))
+        if not self._h:
+            raise EMGError(EMG_ERR_USER, lib().emg_last_error().decode())
+        n = [C.c_int() for _ in range(4)]
+        _check(lib().emg_survey_sizes(self._h, *[C.byref(x) for x in n]))
+        nf, ntx, nrx, nobs = [x.value for x in n]
+        self.freqs = np.zeros(nf)
+        self.tx = np.zeros((ntx, 7))
+        self.rx = np.zeros((nrx, 3))
+        self.otype, self.fidx, self.tidx, self.ridx = (np.zeros(nobs, dtype=np.int32) for _ in range(4))
+        self.obs = np.zeros(nobs, dtype=np.complex128)
+        self.obserr = np.zeros(nobs, dtype=np.complex128)
+        _check(lib().emg_survey_get(self._h, _ptr(self.freqs), _ptr(self.tx), _ptr(self.rx), _ptr(self.otype),
+                                    _ptr(self.fidx), _ptr(self.tidx), _ptr(self.ridx),
+                                    _ptr(self.obs.view(np.float64)), _ptr(self.obserr.view(np.float64))))
+
+    def write_rsp(self, path, rsp):
+        r = np.ascontiguousarray(np.asarray(rsp, dtype=np.complex128).reshape(-1))
+        if r.size != self.obs.size:
+            raise EMGError(EMG_ERR_ARG, "one response per observation")
+        _check(lib().emg_survey_write_rsp(self._h, os.fsencode(path), _ptr(r.view(np.float64))))
+
+    def close(self):
+        if self._h:
+            lib().emg_survey_destroy(self._h)
             self._h = None
 
     def __del__(self):

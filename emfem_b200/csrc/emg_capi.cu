@@ -19,6 +19,7 @@
 #include "emg_kernels.cuh"
 #include "emg_linalg.h"
 #include "emg_locate.h"
+#include "emg_io.h"
 #include "emg_solver.h"
 
 namespace emg {
@@ -1148,6 +1149,75 @@ int emg_find_cell_around_point(emg_context *c, int n, const double *pts, int *te
   locate_all(*c->locator, n, pts, tets_out);
   EMG_API_END
 }
+
+struct emg_survey {
+  emg::Survey s;
+};
+
+emg_survey *emg_survey_read_emd(const char *path) {
+  if (!path) {
+    emg::g_last_error = "null argument";
+    return nullptr;
+  }
+  try {
+    std::unique_ptr<emg_survey> h(new emg_survey);
+    std::string err;
+    if (!emg::read_emd(path, h->s, err)) {
+      emg::g_last_error = err;
+      return nullptr;
+    }
+    return h.release();
+  } catch (const std::exception &e) {
+    emg::g_last_error = e.what();
+  }
+  return nullptr;
+}
+
+int emg_survey_sizes(const emg_survey *h, int *n_freqs, int *n_tx, int *n_rx, int *n_obs) {
+  EMG_API_BEGIN
+  need(h, EMG_ERR_ARG, "null survey");
+  if (n_freqs) *n_freqs = (int)h->s.freqs.size();
+  if (n_tx) *n_tx = (int)h->s.tx.size() / kTxSize;
+  if (n_rx) *n_rx = (int)h->s.rx.size() / 3;
+  if (n_obs) *n_obs = (int)h->s.obs.size();
+  EMG_API_END
+}
+
+int emg_survey_get(const emg_survey *h, double *freqs, double *tx, double *rx, int *otype, int *fidx, int *tidx,
+                   int *ridx, double *obs, double *obserr) {
+  EMG_API_BEGIN
+  need(h, EMG_ERR_ARG, "null survey");
+  const Survey &s = h->s;
+  if (freqs) std::copy(s.freqs.begin(), s.freqs.end(), freqs);
+  if (tx) std::copy(s.tx.begin(), s.tx.end(), tx);
+  if (rx) std::copy(s.rx.begin(), s.rx.end(), rx);
+  if (otype) std::copy(s.otype.begin(), s.otype.end(), otype);
+  if (fidx) std::copy(s.fidx.begin(), s.fidx.end(), fidx);
+  if (tidx) std::copy(s.tidx.begin(), s.tidx.end(), tidx);
+  if (ridx) std::copy(s.ridx.begin(), s.ridx.end(), ridx);
+  for (size_t i = 0; i < s.obs.size(); ++i) {
+    if (obs) {
+      obs[2 * i] = s.obs[i].real();
+      obs[2 * i + 1] = s.obs[i].imag();
+    }
+    if (obserr) {
+      obserr[2 * i] = s.obserr[i].real();
+      obserr[2 * i + 1] = s.obserr[i].imag();
+    }
+  }
+  EMG_API_END
+}
+
+int emg_survey_write_rsp(const emg_survey *h, const char *path, const double *rsp) {
+  EMG_API_BEGIN
+  need(h && path && (rsp || h->s.obs.empty()), EMG_ERR_ARG, "null argument");
+  std::string err;
+  if (!emg::write_rsp(path, h->s, reinterpret_cast<const std::complex<double> *>(rsp), err))
+    fail(EMG_ERR_USER, "%s", err.c_str());
+  EMG_API_END
+}
+
+void emg_survey_destroy(emg_survey *h) { delete h; }
 
 // calculate_response_mt (em_fwd.cc:747-800): the reference's tensor
 // impedance and tipper formulas per observation, plus apparent resistivity

@@ -225,6 +225,23 @@ int emg_calculate_response_mt(double freq, int nrx, const double *fields, int no
 int emg_calculate_response_csem(int nrx, const double *fields, int nobs, const int *otype, const int *ridx,
                                 double *rsp);
 
+/* Survey files in the reference's layout: read_emd (src/em_io.cc:202-287)
+ * and save_rsp (src/em_io.cc:316-399).  emg_survey_read_emd returns NULL on
+ * error (emg_last_error() says why).  Observations come back as the
+ * reference stores them: AP types as (log amplitude, phase in radians) with
+ * errors ((err_amp/100)^2, (err_phase in radians)^2), the others as
+ * (re, im) with squared errors.  emg_survey_write_rsp writes the file with
+ * the responses rsp (one complex value per observation, interleaved, in the
+ * same convention: what emg_calculate_response_mt/csem return).  Host only. */
+typedef struct emg_survey emg_survey;
+emg_survey *emg_survey_read_emd(const char *path);
+int emg_survey_sizes(const emg_survey *s, int *n_freqs, int *n_tx, int *n_rx, int *n_obs);
+/* any output pointer may be NULL; tx holds 7 values per transmitter (TX_SIZE) */
+int emg_survey_get(const emg_survey *s, double *freqs, double *tx, double *rx, int *otype, int *fidx, int *tidx,
+                   int *ridx, double *obs, double *obserr);
+int emg_survey_write_rsp(const emg_survey *s, const char *path, const double *rsp);
+void emg_survey_destroy(emg_survey *s);
+
 /* ---- batched fast path (no reference counterpart: replaces the per-task
  * loop of forward_mt/forward_csem, src/em_fwd.cc:1320-1439) -------------
  * Solves k right-hand sides with individual frequencies as one block:
