@@ -103,3 +103,61 @@ def test_refine_marking_matches_oracle(seed):
         assert np.array_equal(E.refine_fixed_number(err, frac), O.refine_fixed_number(err, frac))
     with pytest.raises(E.EMGError):
         E.refine_fixed_number(err, 1.5)
+
+
+C_CLIENT = r"""
+#include <stdio.h>
+#include "emfem_b200.h"
+/* two tets sharing the face (1,2,3): (0,1,2,3) and (4,1,3,2) */
+static const double pts[15] = {0,0,0, 1,0,0, 0,1,0, 0,0,1, 1,1,1};
+static const int tets[8] = {0,1,2,3, 4,1,3,2};
+static const int nbr[8] = {-1,-1,-1,1, -1,-1,-1,0};
+int main(int argc, char **argv) {
+  const double q[9] = {0.1,0.1,0.1, 0.6,0.6,0.6, 5,5,5};
+  int t[3] = {-9,-9,-9};
+  emg_point_index *ix = emg_point_index_create(5, pts, 2, tets, nbr);
+  if (!ix || emg_point_index_find(ix, 3, q, t) != EMG_OK) return 1;
+  emg_point_index_destroy(ix);
+  emg_survey *s = emg_survey_read_emd(argv[1]);
+  if (!s) { printf("%s\n", emg_last_error()); return 2; }
+  int nf, ntx, nrx, nobs;
+  emg_survey_sizes(s, &nf, &ntx, &nrx, &nobs);
+  int ot[4], ri[4];
+  emg_survey_get(s, 0, 0, 0, ot, 0, 0, ri, 0, 0);
+  double f[24] = {0}, rsp[8];
+  f[0] = 1.0; f[8] = 1.0; f[14] = 2.0; f[18] = -1.0;  /* Ex, Hy (XY), Ey, Hx (YX) */
+  if (emg_calculate_response_mt(1.0, nrx, f, nobs, ot, ri, rsp) != EMG_OK) return 3;
+  if (emg_survey_write_rsp(s, argv[2], rsp) != EMG_OK) return 4;
+  emg_survey_destroy(s);
+  printf("%d %d %d %d %d %.6f %.6f\n", t[0], t[1], t[2], nobs, ot[0], rsp[0], rsp[2]);
+  return 0;
+}
+"""
+
+
+def test_c_client_uses_the_abi(tmp_path):
+    """A plain C99 program compiled against include/emfem_b200.h and linked to
+    the library uses the host-only entry points (point location, survey files,
+    responses) without a GPU."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "client.c"
+    src.write_text(C_CLIENT)
+    exe = tmp_path / "client"
+    libdir = os.path.dirname(E.library_path())
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(root, "include"), str(src),
+                    "-L", libdir, "-lemfem_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    emd = tmp_path / "s.emd"
+    emd.write_text("1\n1.0\n0\n1\n0 0 0\n2\n321 0 -3 0 1 0 0.1 0.1\n331 0 -3 0 1 0 0.1 0.1\n")
+    out = subprocess.run([str(exe), str(emd), str(tmp_path / "s.rsp")], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    t0, t1, t2, nobs, ot0, z_xy, z_yx = out.stdout.split()
+    assert (int(t0), int(t1), int(t2)) == (0, 1, -1)
+    assert int(nobs) == 2 and int(ot0) == 321
+    # 1-D fields: Z_XY = Ex / Hy = 1, Z_YX = Ey / Hx = -2
+    assert float(z_xy) == 1.0 and float(z_yx) == -2.0
+    assert (tmp_path / "s.rsp").read_text().startswith("# frequencies\n1\n")
