@@ -170,85 +170,135 @@ static void direct_interp(const HCsr &A, double w, const std::vector<int> &fn, c
     if (cf[i] == 1) cidx[i] = nc++;
   P.n = n;
   P.m = nc;
-  std::vector<std::vector<std::pair<int, double>>> rows(n);
+  // row i of P into `row` (sorted by coarse column); `strong` is a zeroed
+  // marker array of n entries, returned zeroed
+  auto make_row = [&](int i, std::vector<char> &strong, std::vector<std::pair<int, double>> &row) {
+    row.clear();
+    if (cf[i] == 1) {
+      row.push_back({cidx[i], 1.0});
+      return;
+    }
+    for (int k = srp[i]; k < srp[i + 1]; ++k) strong[sci[k]] = 1;
+    double diag = 0, sn = 0, sp = 0, cn = 0, cp = 0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int j = A.ci[k];
+      double a = combined(A, k, w);
+      if (j == i) { diag = a; continue; }
+      if (!same_fn(fn, i, j)) continue;
+      if (a < 0) sn += a; else sp += a;
+      if (cf[j] == 1 && strong[j]) { if (a < 0) cn += a; else cp += a; }
+    }
+    double alpha = cn != 0 ? sn / cn : 0.0;
+    double beta = cp != 0 ? sp / cp : 0.0;
+    if (cp == 0) diag += sp;
+    if (diag != 0) {
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        if (j == i || cf[j] != 1 || !strong[j]) continue;
+        double a = combined(A, k, w);
+        row.push_back({cidx[j], -(a < 0 ? alpha : beta) * a / diag});
+      }
+    }
+    for (int k = srp[i]; k < srp[i + 1]; ++k) strong[sci[k]] = 0;
+    if ((int)row.size() > pmax) {
+      double tot = 0, kept = 0;
+      for (auto &p : row) tot += p.second;
+      std::partial_sort(row.begin(), row.begin() + pmax, row.end(),
+                        [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+                          return std::fabs(a.second) > std::fabs(b.second);
+                        });
+      row.resize(pmax);
+      for (auto &p : row) kept += p.second;
+      if (kept != 0)
+        for (auto &p : row) p.second *= tot / kept;
+    }
+    std::sort(row.begin(), row.end());
+  };
+  // two passes over the rows (sizes, then entries) with per-thread scratch:
+  // no per-row allocation; each row is computed the same way both times
+  P.rp.assign(n + 1, 0);
 #pragma omp parallel
   {
     std::vector<char> strong(n, 0);
+    std::vector<std::pair<int, double>> row;
 #pragma omp for schedule(dynamic, 1024)
     for (int i = 0; i < n; ++i) {
-      auto &row = rows[i];
-      if (cf[i] == 1) {
-        row.push_back({cidx[i], 1.0});
-        continue;
-      }
-      for (int k = srp[i]; k < srp[i + 1]; ++k) strong[sci[k]] = 1;
-      double diag = 0, sn = 0, sp = 0, cn = 0, cp = 0;
-      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-        int j = A.ci[k];
-        double a = combined(A, k, w);
-        if (j == i) { diag = a; continue; }
-        if (!same_fn(fn, i, j)) continue;
-        if (a < 0) sn += a; else sp += a;
-        if (cf[j] == 1 && strong[j]) { if (a < 0) cn += a; else cp += a; }
-      }
-      double alpha = cn != 0 ? sn / cn : 0.0;
-      double beta = cp != 0 ? sp / cp : 0.0;
-      if (cp == 0) diag += sp;
-      if (diag != 0) {
-        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-          int j = A.ci[k];
-          if (j == i || cf[j] != 1 || !strong[j]) continue;
-          double a = combined(A, k, w);
-          row.push_back({cidx[j], -(a < 0 ? alpha : beta) * a / diag});
-        }
-      }
-      for (int k = srp[i]; k < srp[i + 1]; ++k) strong[sci[k]] = 0;
-      if ((int)row.size() > pmax) {
-        double tot = 0, kept = 0;
-        for (auto &p : row) tot += p.second;
-        std::partial_sort(row.begin(), row.begin() + pmax, row.end(),
-                          [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
-                            return std::fabs(a.second) > std::fabs(b.second);
-                          });
-        row.resize(pmax);
-        for (auto &p : row) kept += p.second;
-        if (kept != 0)
-          for (auto &p : row) p.second *= tot / kept;
-      }
-      std::sort(row.begin(), row.end());
+      make_row(i, strong, row);
+      P.rp[i + 1] = (int)row.size();
     }
   }
-  P.rp.assign(n + 1, 0);
-  for (int i = 0; i < n; ++i) P.rp[i + 1] = P.rp[i] + (int)rows[i].size();
+  for (int i = 0; i < n; ++i) P.rp[i + 1] += P.rp[i];
   P.ci.resize(P.rp[n]);
   P.vc.resize(P.rp[n]);
   P.vm.clear();
-  for (int i = 0; i < n; ++i)
-    for (size_t k = 0; k < rows[i].size(); ++k) {
-      P.ci[P.rp[i] + k] = rows[i][k].first;
-      P.vc[P.rp[i] + k] = rows[i][k].second;
+#pragma omp parallel
+  {
+    std::vector<char> strong(n, 0);
+    std::vector<std::pair<int, double>> row;
+#pragma omp for schedule(dynamic, 1024)
+    for (int i = 0; i < n; ++i) {
+      make_row(i, strong, row);
+      for (size_t k = 0; k < row.size(); ++k) {
+        P.ci[P.rp[i] + k] = row[k].first;
+        P.vc[P.rp[i] + k] = row[k].second;
+      }
     }
+  }
 }
 
+// A^T with the entries of every row in increasing column order of A (the
+// order a serial row-by-row scatter gives): rows of A are split into one
+// contiguous chunk per thread, and each thread scatters its chunk behind the
+// entries of the chunks before it.
 HCsr transpose(const HCsr &A) {
   HCsr T;
   T.n = A.m;
   T.m = A.n;
+  const long nnz = A.nnz();
+  const bool two = !A.vm.empty();
   T.rp.assign(T.n + 1, 0);
-  long nnz = A.nnz();
-  for (long k = 0; k < nnz; ++k) T.rp[A.ci[k] + 1]++;
-  for (int i = 0; i < T.n; ++i) T.rp[i + 1] += T.rp[i];
   T.ci.resize(nnz);
   T.vc.resize(nnz);
-  if (!A.vm.empty()) T.vm.resize(nnz);
-  std::vector<int> pos(T.rp.begin(), T.rp.end() - 1);
-  for (int i = 0; i < A.n; ++i)
-    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-      int p = pos[A.ci[k]]++;
-      T.ci[p] = i;
-      T.vc[p] = A.vc[k];
-      if (!A.vm.empty()) T.vm[p] = A.vm[k];
+  if (two) T.vm.resize(nnz);
+#ifdef _OPENMP
+  const int nth = std::max(1, std::min(omp_get_max_threads(), (int)(nnz / 65536) + 1));
+#else
+  const int nth = 1;
+#endif
+  std::vector<std::vector<int>> cnt(nth, std::vector<int>(T.n, 0));
+  auto chunk = [&](int t, int &r0, int &r1) {
+    r0 = (int)((long)A.n * t / nth);
+    r1 = (int)((long)A.n * (t + 1) / nth);
+  };
+#pragma omp parallel for num_threads(nth) schedule(static, 1)
+  for (int t = 0; t < nth; ++t) {
+    int r0, r1;
+    chunk(t, r0, r1);
+    for (long k = A.rp[r0]; k < A.rp[r1]; ++k) cnt[t][A.ci[k]]++;
+  }
+  for (int c = 0; c < T.n; ++c) {
+    int tot = 0;
+    for (int t = 0; t < nth; ++t) {
+      const int v = cnt[t][c];
+      cnt[t][c] = tot;  // offset of thread t inside row c
+      tot += v;
     }
+    T.rp[c + 1] = T.rp[c] + tot;
+  }
+#pragma omp parallel for num_threads(nth) schedule(static, 1)
+  for (int t = 0; t < nth; ++t) {
+    int r0, r1;
+    chunk(t, r0, r1);
+    std::vector<int> &pos = cnt[t];
+    for (int i = r0; i < r1; ++i)
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        const int c = A.ci[k];
+        const int p = T.rp[c] + pos[c]++;
+        T.ci[p] = i;
+        T.vc[p] = A.vc[k];
+        if (two) T.vm[p] = A.vm[k];
+      }
+  }
   return T;
 }
 
@@ -322,34 +372,28 @@ HCsr galerkin(const HCsr &R, const HCsr &A, const HCsr &P) {
   C.n = R.n;
   C.m = P.m;
   const bool two = !A.vm.empty();
-  std::vector<int> cnt(C.n + 1, 0);
-#pragma omp parallel
+  // one pass: each thread appends its rows to its own arena (columns sorted,
+  // values summed in the order R's, A's and P's entries are met); the rows
+  // are then copied into place
+  struct Arena {
+    std::vector<int> ci;
+    std::vector<double> vc, vm;
+  };
+#ifdef _OPENMP
+  const int nth = omp_get_max_threads();
+#else
+  const int nth = 1;
+#endif
+  std::vector<Arena> arena(nth);
+  std::vector<int> owner(C.n), start(C.n), len(C.n);
+#pragma omp parallel num_threads(nth)
   {
-    std::vector<int> mark(P.m, -1);
-#pragma omp for schedule(dynamic, 64)
-    for (int I = 0; I < C.n; ++I) {
-      int c = 0;
-      for (int kr = R.rp[I]; kr < R.rp[I + 1]; ++kr) {
-        const int i = R.ci[kr];
-        for (int ka = A.rp[i]; ka < A.rp[i + 1]; ++ka) {
-          const int k = A.ci[ka];
-          for (int kp = P.rp[k]; kp < P.rp[k + 1]; ++kp)
-            if (mark[P.ci[kp]] != I) {
-              mark[P.ci[kp]] = I;
-              ++c;
-            }
-        }
-      }
-      cnt[I + 1] = c;
-    }
-  }
-  C.rp.assign(C.n + 1, 0);
-  for (int I = 0; I < C.n; ++I) C.rp[I + 1] = C.rp[I] + cnt[I + 1];
-  C.ci.resize(C.rp[C.n]);
-  C.vc.resize(C.rp[C.n]);
-  if (two) C.vm.resize(C.rp[C.n]);
-#pragma omp parallel
-  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num();
+#else
+    const int tid = 0;
+#endif
+    Arena &ar = arena[tid];
     std::vector<int> mark(P.m, -1);
     std::vector<double> ac(P.m), am(two ? P.m : 0);
     std::vector<int> cols;
@@ -376,21 +420,33 @@ HCsr galerkin(const HCsr &R, const HCsr &A, const HCsr &P) {
         }
       }
       std::sort(cols.begin(), cols.end());
-      int p = C.rp[I];
+      owner[I] = tid;
+      start[I] = (int)ar.ci.size();
+      len[I] = (int)cols.size();
       for (int J : cols) {
-        C.ci[p] = J;
-        C.vc[p] = ac[J];
-        if (two) C.vm[p] = am[J];
-        ++p;
+        ar.ci.push_back(J);
+        ar.vc.push_back(ac[J]);
+        if (two) ar.vm.push_back(am[J]);
       }
     }
+  }
+  C.rp.assign(C.n + 1, 0);
+  for (int I = 0; I < C.n; ++I) C.rp[I + 1] = C.rp[I] + len[I];
+  C.ci.resize(C.rp[C.n]);
+  C.vc.resize(C.rp[C.n]);
+  if (two) C.vm.resize(C.rp[C.n]);
+#pragma omp parallel for schedule(static)
+  for (int I = 0; I < C.n; ++I) {
+    const Arena &ar = arena[owner[I]];
+    std::copy(ar.ci.begin() + start[I], ar.ci.begin() + start[I] + len[I], C.ci.begin() + C.rp[I]);
+    std::copy(ar.vc.begin() + start[I], ar.vc.begin() + start[I] + len[I], C.vc.begin() + C.rp[I]);
+    if (two) std::copy(ar.vm.begin() + start[I], ar.vm.begin() + start[I] + len[I], C.vm.begin() + C.rp[I]);
   }
   return C;
 }
 
-void amg_build(const HCsr &A0, double w_ref, const AmgParams &prm, HostAmg &out) {
+void amg_build(HCsr A, double w_ref, const AmgParams &prm, HostAmg &out) {
   out.lv.clear();
-  HCsr A = A0;
   std::vector<int> fn;
   if (prm.num_functions > 1) {
     fn.resize(A.n);

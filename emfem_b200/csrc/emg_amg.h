@@ -33,7 +33,8 @@ struct HostAmg {
 HCsr transpose(const HCsr &A);
 HCsr spgemm(const HCsr &A, const HCsr &B);
 HCsr galerkin(const HCsr &R, const HCsr &A, const HCsr &P);
-void amg_build(const HCsr &A0, double w_ref, const AmgParams &prm, HostAmg &out);
+// builds the hierarchy of A (taken by value: pass an rvalue to avoid a copy)
+void amg_build(HCsr A, double w_ref, const AmgParams &prm, HostAmg &out);
 void coarse_inverse(const HCsr &A, double w, std::vector<double> &X);
 
 }  // namespace emg

@@ -259,7 +259,7 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
     p2.seed = prm.seed + 7919ull * (uint64_t)sp;
     p2.num_functions = sp == SUB_PIVEC ? 3 : 1;
     auto ta = std::chrono::steady_clock::now();
-    amg_build(nod[sp], w_ref, p2, hamg);
+    amg_build(std::move(nod[sp]), w_ref, p2, hamg);
     auto tb = std::chrono::steady_clock::now();
     amg_ms += std::chrono::duration<double, std::milli>(tb - ta).count();
     S.lv.resize(hamg.lv.size());
