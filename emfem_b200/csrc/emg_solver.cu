@@ -62,22 +62,35 @@ __global__ void fcg_alpha_kernel(int K, const double *__restrict__ dots, double 
 }
 
 template <typename T>
+static void convert(const std::vector<double> &a, std::vector<T> &b) {
+  b.resize(a.size());
+  const long n = (long)a.size();
+#pragma omp parallel for schedule(static)
+  for (long k = 0; k < n; ++k) b[k] = (T)a[k];
+}
+
+template <typename T>
 static void upload_csr(const HCsr &h, DCsr<T> &d, bool with_l1, cudaStream_t s) {
   d.n = h.n;
   d.m = h.m;
   d.nnz = h.nnz();
   d.rp.upload(h.rp, s);
   d.ci.upload(h.ci, s);
-  std::vector<T> tmp(h.vc.begin(), h.vc.end());
+  std::vector<T> tmp;
+  convert(h.vc, tmp);
   d.vc.upload(tmp, s);
+  std::vector<T> tm;
   if (!h.vm.empty()) {
-    std::vector<T> tm(h.vm.begin(), h.vm.end());
+    convert(h.vm, tm);
     d.vm.upload(tm, s);
   } else {
     d.vm.release();
   }
+  std::vector<T> lc, lm;
   if (with_l1) {
-    std::vector<T> lc(h.n), lm(h.vm.empty() ? 0 : h.n);
+    lc.resize(h.n);
+    lm.resize(h.vm.empty() ? 0 : h.n);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < h.n; ++i) {
       double a = 0, b = 0;
       for (int k = h.rp[i]; k < h.rp[i + 1]; ++k) {
