@@ -450,16 +450,17 @@ void assemble_nodal(Context &c, HCsr out[4]) {
   for (int k = 0; k < 8; ++k) o.v[k] = buf.p + (size_t)k * vnnz;
   assemble_nodal_kernel<<<(unsigned)((c.nt + 127) / 128), 128, 0, c.stream>>>(elem_in(c), c.nt, c.vslot.p, o);
   EMG_LAUNCH_CHECK();
-  std::vector<double> h((size_t)vnnz * 8);
-  buf.download(h.data(), h.size(), c.stream);
-  EMG_CUDA(cudaStreamSynchronize(c.stream));
+  // each part straight into its operator (no staging copy of all eight)
   for (int sp = 0; sp < 4; ++sp) {
     out[sp].n = out[sp].m = c.nv;
     out[sp].rp = c.h_vrp;
     out[sp].ci = c.h_vci;
-    out[sp].vc.assign(h.begin() + (size_t)(2 * sp) * vnnz, h.begin() + (size_t)(2 * sp + 1) * vnnz);
-    out[sp].vm.assign(h.begin() + (size_t)(2 * sp + 1) * vnnz, h.begin() + (size_t)(2 * sp + 2) * vnnz);
+    out[sp].vc.resize(vnnz);
+    out[sp].vm.resize(vnnz);
+    buf.download_at(out[sp].vc.data(), (size_t)(2 * sp) * vnnz, vnnz, c.stream);
+    buf.download_at(out[sp].vm.data(), (size_t)(2 * sp + 1) * vnnz, vnnz, c.stream);
   }
+  EMG_CUDA(cudaStreamSynchronize(c.stream));
 }
 
 // The vector nodal space of AMS (hypre's Pi space, cycle character '2'):

@@ -101,6 +101,11 @@ struct DBuf {
   void download(T *h, size_t count, cudaStream_t s) const {
     if (count) EMG_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
   }
+  // count elements starting at element offset
+  void download_at(T *h, size_t offset, size_t count, cudaStream_t s) const {
+    if (offset + count > n) fail(EMG_ERR_ARG, "download past the end of a device buffer");
+    if (count) EMG_CUDA(cudaMemcpyAsync(h, p + offset, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
   void zero(cudaStream_t s) {
     if (n) EMG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
   }
