@@ -4,8 +4,8 @@
 Workload (default): the batched + mixed-precision MT configuration with
 topography -- ~1.5M tets, 8 frequencies log-spaced in [1e-3, 100] Hz x 2
 polarisations = 16 right-hand sides solved as one block (synthetic seeded
-mesh/model from emfem_b200.meshgen).  One step = the hot path
-over that batch: assemble_matrix, AMS setup, MT right-hand sides, block
+mesh/model from emfem_b200.meshgen).  One step = the hot path over that
+batch: assemble_matrix, AMS setup, MT right-hand sides, block
 FGMRES(FCG(AMS)) solve with FP64 outer iterations and an FP32 AMS.
 
 value  : RHS/s with inputs resident on the device (device-timed, CUDA events)
@@ -13,8 +13,10 @@ e2e    : RHS/s through the host-buffer C ABI (emg_assemble_rhs_mt_block +
          emg_solve_block), host<->device copies inside the timed region
 plain_fp64 : the per-RHS FP64 drop-in (real-form FGMRES, per-frequency AMS
          setup, zero guess) on a subset of the same columns, for the ratio
-roofline : the edge-operator SpMM inside the AMS (dominant kernel), achieved
-         algorithmic GB/s from live CUDA-event profiling over the timed region
+roofline : the edge-level FP32 SpMM inside the AMS (the launch shape with
+         the largest share of device time), achieved algorithmic GB/s from
+         CUDA events around its launches in one profiled step after the timed
+         region; traffic from the committed ncu capture's traffic ratio
 cpu_baseline : the CPU oracle (restatement of the reference path) on a bounded
          sample of the same workload, rank 0, N=1 only
 
