@@ -617,8 +617,7 @@ int emg_set_mesh(emg_context *c, int nv, const double *pts, int nt, const int *t
   EMG_API_BEGIN
   need(c && pts && tets && attr && edges && t2e && nbr && non && ebdr, EMG_ERR_ARG, "null mesh array");
   need(nv > 0 && nt > 0 && ne > 0, EMG_ERR_ARG, "empty mesh");
-  need(c->device >= 0, EMG_ERR_STATE, "host-only context has no device");
-  EMG_CUDA(cudaSetDevice(c->device));
+  if (c->device >= 0) EMG_CUDA(cudaSetDevice(c->device));
   for (long i = 0; i < 4L * nt; ++i)
     need(tets[i] >= 0 && tets[i] < nv, EMG_ERR_ARG, "tetrahedronlist index out of range");
   for (long i = 0; i < 6L * nt; ++i) need(t2e[i] >= 0 && t2e[i] < ne, EMG_ERR_ARG, "tet2edgelist index out of range");
@@ -642,6 +641,12 @@ int emg_set_mesh(emg_context *c, int nv, const double *pts, int nt, const int *t
   c->bnd_rank.release();
   c->tiles.clear();
   c->locator.reset();
+  c->have_ls = false;
+  c->assembled = false;
+  c->have_pc = false;
+  c->ws->block_ready64 = c->ws->block_ready32 = false;
+  c->sol.clear();
+  if (c->device < 0) return EMG_OK;  // host-only context: host-side entry points only
   c->pts.upload(c->h_pts, c->stream);
   c->tets.upload(c->h_tets, c->stream);
   c->attr.upload(c->h_attr, c->stream);
@@ -651,11 +656,6 @@ int emg_set_mesh(emg_context *c, int nv, const double *pts, int nt, const int *t
   c->non.upload(c->h_non, c->stream);
   c->ebdr.upload(c->h_ebdr, c->stream);
   canonicalize(*c);
-  c->have_ls = false;
-  c->assembled = false;
-  c->have_pc = false;
-  c->ws->block_ready64 = c->ws->block_ready32 = false;
-  c->sol.clear();
   EMG_CUDA(cudaStreamSynchronize(c->stream));
   EMG_API_END
 }
@@ -688,10 +688,16 @@ int emg_set_frequencies(emg_context *c, int n, const double *f) {
   EMG_API_END
 }
 
+// makes the context's GPU current; a host-only context (device -1) refuses
+static void use_device(const Context &c) {
+  need(c.device >= 0, EMG_ERR_STATE, "host-only context has no device");
+  EMG_CUDA(cudaSetDevice(c.device));
+}
+
 int emg_create_linear_system(emg_context *c, int tidx) {
   EMG_API_BEGIN
   need(c && c->nt > 0, EMG_ERR_STATE, "create_linear_system before emg_set_mesh");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   c->tidx = tidx;
   c->tiles.clear();
   build_sparsity(*c);
@@ -746,7 +752,7 @@ int emg_assemble_matrix(emg_context *c, int fidx) {
   need(c && c->have_ls, EMG_ERR_STATE, "assemble_matrix before create_linear_system");
   need(c->nrho > 0, EMG_ERR_STATE, "assemble_matrix before emg_set_model");
   need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   c->omega = 2 * PI * c->freqs[fidx];
   cudaEvent_t e0, e1;
   EMG_CUDA(cudaEventCreate(&e0));
@@ -774,7 +780,7 @@ __global__ static void scale_copy_kernel(long n, const double *a, double w, doub
 int emg_get_matrices(emg_context *c, double *C, double *M, unsigned char *bdr) {
   EMG_API_BEGIN
   need(c && c->assembled, EMG_ERR_STATE, "matrices not assembled");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   if (C) c->Cv.download(C, c->nnz, c->stream);
   if (M) {
     DBuf<double> tmp(c->nnz);
@@ -791,7 +797,7 @@ int emg_get_matrices(emg_context *c, double *C, double *M, unsigned char *bdr) {
 int emg_create_pc(emg_context *c) {
   EMG_API_BEGIN
   need(c && c->assembled, EMG_ERR_STATE, "create_pc before assemble_matrix");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   cudaEvent_t e0, e1;
   EMG_CUDA(cudaEventCreate(&e0));
   EMG_CUDA(cudaEventCreate(&e1));
@@ -822,7 +828,7 @@ int emg_matshell_mult_a(emg_context *c, const double *x, double *y) {
   EMG_API_BEGIN
   need(c && x && y, EMG_ERR_ARG, "null argument");
   need(c->assembled, EMG_ERR_STATE, "operator not assembled");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   const int n = c->ne;
   std::vector<double> xi = interleave(x, x + n, n);
   Workspace &w = *c->ws;
@@ -845,7 +851,7 @@ int emg_pc_apply_b(emg_context *c, const double *b, double *x) {
   EMG_API_BEGIN
   need(c && b && x, EMG_ERR_ARG, "null argument");
   need(c->have_pc, EMG_ERR_STATE, "pc_apply_b before create_pc");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   const int n = c->ne;
   Workspace &w = *c->ws;
   std::vector<double> bi = interleave(b, b + n, n);
@@ -879,7 +885,7 @@ int emg_solve_linear_system(emg_context *c, int target, const double *s_re, cons
   need(c && s_re && s_im, EMG_ERR_ARG, "null argument");
   need(c->have_pc, EMG_ERR_STATE, "solve_linear_system before create_pc");
   need(max_it > 0 && rtol > 0, EMG_ERR_ARG, "bad tolerances");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   const int n = c->ne;
   Workspace &w = *c->ws;
   DBuf<double> &x = slot_buf(*c, target);
@@ -908,7 +914,7 @@ int emg_get_solution(emg_context *c, int target, double *e_re, double *e_im) {
   EMG_API_BEGIN
   need(c && (e_re || e_im), EMG_ERR_ARG, "null argument");
   need(c->have_ls, EMG_ERR_STATE, "no linear system");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   DBuf<double> &x = slot_buf(*c, target);
   std::vector<double> v((size_t)c->ne * 2);
   x.download(v.data(), v.size(), c->stream);
@@ -924,7 +930,7 @@ int emg_set_solution(emg_context *c, int target, const double *e_re, const doubl
   EMG_API_BEGIN
   need(c && e_re && e_im, EMG_ERR_ARG, "null argument");
   need(c->have_ls, EMG_ERR_STATE, "no linear system");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   DBuf<double> &x = slot_buf(*c, target);
   std::vector<double> v = interleave(e_re, e_im, c->ne);
   x.upload(v, c->stream);
@@ -989,7 +995,7 @@ int emg_assemble_rhs_mt(emg_context *c, int fidx, int mode, double *s_re, double
   need(c->assembled, EMG_ERR_STATE, "assemble_rhs_mt before assemble_matrix");
   need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
   need(mode == EMG_SOL_MT_XY || mode == EMG_SOL_MT_YX, EMG_ERR_ARG, "mode must be XY_POLAR or YX_POLAR");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   DBuf<double> s((size_t)c->ne * 2);
   double f = c->freqs[fidx];
   rhs_mt_block(*c, 1, &f, &mode, s.p);
@@ -1074,7 +1080,7 @@ int emg_estimate_error(emg_context *c, int fidx, int tidx, double *err, double *
   need(c && (err || eta_raw), EMG_ERR_ARG, "null argument");
   need(c->have_ls && c->nrho > 0, EMG_ERR_STATE, "estimate_error before create_linear_system");
   need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   Workspace &w = *c->ws;
   std::vector<int> slots = tidx < 0 ? std::vector<int>{EMG_SOL_MT_XY, EMG_SOL_MT_YX, EMG_SOL_DUAL}
                                     : std::vector<int>{EMG_SOL_CSEM, EMG_SOL_DUAL};
@@ -1331,7 +1337,7 @@ int emg_interpolate_fields(emg_context *c, int target, int fidx, int n, const do
   EMG_API_BEGIN
   need(c && pts && tets && eh, EMG_ERR_ARG, "null argument");
   need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   DBuf<double> &x = slot_buf(*c, target);
   std::vector<double> v((size_t)c->ne * 2);
   x.download(v.data(), v.size(), c->stream);
@@ -1500,7 +1506,7 @@ int emg_solve_block_dev(emg_context *c, int k, const double *freqs, const double
                         const emg_block_opts *opts, emg_solve_info *infos) {
   EMG_API_BEGIN
   need(c && freqs && rhs_dev && x_dev && opts, EMG_ERR_ARG, "null argument");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   solve_block_dev(*c, k, freqs, rhs_dev, x_dev, *opts, infos);
   EMG_API_END
 }
@@ -1509,7 +1515,7 @@ int emg_solve_block(emg_context *c, int k, const double *freqs, const double *rh
                     const emg_block_opts *opts, emg_solve_info *infos) {
   EMG_API_BEGIN
   need(c && freqs && rhs && x && opts, EMG_ERR_ARG, "null argument");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   const size_t N = (size_t)c->ne * k * 2;
   DBuf<double> b(N), xd(N);
   b.upload(rhs, N, c->stream);
@@ -1525,7 +1531,7 @@ int emg_spmv_complex_dev(emg_context *c, int k, const double *omegas, const doub
   EMG_API_BEGIN
   need(c && omegas && x_dev && y_dev, EMG_ERR_ARG, "null argument");
   need(c->assembled, EMG_ERR_STATE, "operator not assembled");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   c->ws->omega_k.upload(omegas, k, c->stream);
   spmm_complex(c->ne, k, c->rp.p, c->ci.p, c->Cv.p, c->Msv.p, c->ws->omega_k.p, x_dev, nullptr, y_dev, false,
                conj_out != 0, c->stream);
@@ -1583,7 +1589,7 @@ int emg_assemble_rhs_mt_block_dev(emg_context *c, int k, const double *freqs, co
   need(c->assembled, EMG_ERR_STATE, "assemble_rhs_mt before assemble_matrix");
   for (int j = 0; j < k; ++j)
     need(modes[j] == EMG_SOL_MT_XY || modes[j] == EMG_SOL_MT_YX, EMG_ERR_ARG, "mode must be XY_POLAR or YX_POLAR");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   rhs_mt_block(*c, k, freqs, modes, s_dev);
   EMG_API_END
 }
@@ -1592,7 +1598,7 @@ int emg_assemble_rhs_mt_block(emg_context *c, int k, const double *freqs, const 
   EMG_API_BEGIN
   need(c && freqs && modes && s && k > 0, EMG_ERR_ARG, "null argument");
   need(c->assembled, EMG_ERR_STATE, "assemble_rhs_mt before assemble_matrix");
-  EMG_CUDA(cudaSetDevice(c->device));
+  use_device(*c);
   DBuf<double> d((size_t)c->ne * k * 2);
   rhs_mt_block(*c, k, freqs, modes, d.p);
   d.download(s, (size_t)c->ne * k * 2, c->stream);

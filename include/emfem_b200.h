@@ -54,7 +54,11 @@ typedef struct emg_solve_info {
 const char *emg_last_error(void);
 const char *emg_version(void);
 
-/* create_context / destroy_context (src/em_ctx.cc:7-98). device: CUDA ordinal. */
+/* create_context / destroy_context (src/em_ctx.cc:7-98). device: CUDA ordinal,
+ * or -1 for a host-only context: it takes options, mesh, model, frequencies
+ * and background, and serves the host-side entry points (CSEM and dual
+ * right-hand sides, point location, marking, responses); every entry point
+ * that needs a GPU returns EMG_ERR_STATE. */
 int emg_create_context(emg_context **ctx, int device);
 int emg_destroy_context(emg_context *ctx);
 

@@ -86,11 +86,49 @@ def test_host_only_context_refuses_device_work():
     with E.EMContext(-1) as c:
         from emfem_b200 import meshgen as mg
         prob = mg.mt_halfspace_block(800, freqs=(1.0,))
-        with pytest.raises(E.EMGError) as ei:
-            c.set_mesh(prob.mesh)
-        assert ei.value.code == E.api.EMG_ERR_STATE
-        with pytest.raises(E.EMGError):
-            c.create_linear_system(-3)
+        c.set_mesh(prob.mesh)      # host arrays only
+        for call in (lambda: c.create_linear_system(-3), lambda: c.assemble_matrix(0)):
+            with pytest.raises(E.EMGError) as ei:
+                call()
+            assert ei.value.code == E.api.EMG_ERR_STATE
+
+
+def test_host_only_context_rhs_and_location():
+    """A context without a GPU (device -1) holds the mesh on the host and
+    serves the host-side entry points: CSEM and dual right-hand sides
+    (assemble_rhs_csem / assemble_rhs_dual, src/em_fwd.cc:582-717) against
+    the oracle to 1e-12 of the largest entry, and point location on the
+    context's mesh against the oracle's walk (identical tets)."""
+    from emfem_b200 import meshgen as mg
+    prob = mg.marine_csem(3000, freqs=(0.25, 1.25), name="csem-host")
+    om = O.Mesh(prob.mesh)
+    with E.EMContext(-1) as c:
+        c.set_mesh(prob.mesh)
+        c.set_model(prob.model)
+        c.set_frequencies(prob.survey.freqs)
+        rx = prob.survey.rx
+        tets = c.find_cell_around_point(rx)
+        assert np.array_equal(tets, O.find_cell(om, rx)) and (tets >= 0).all()
+        sr, si = c.assemble_rhs_dual(rx, tets)
+        osr, osi = O.rhs_dual(om, rx)
+        assert np.abs(sr - osr).max() <= 1e-12 * np.abs(osr).max()
+        assert np.abs(si - osi).max() <= 1e-12 * np.abs(osi).max()
+        point = np.array(prob.survey.tx[0], dtype=np.float64)
+        line = point.copy()
+        line[3], line[6] = 30.0, 250.0  # a 250 m line source at azimuth 30 degrees
+        for tx, (fidx, f) in ((point, (0, prob.survey.freqs[0])), (line, (1, prob.survey.freqs[1]))):
+            if abs(tx[6]) <= 0.1:
+                pts = tx[None, :3]
+            else:  # the line source split into n_tx_divisions dipoles (default 20)
+                d = np.array([np.cos(np.radians(tx[3])) * np.cos(np.radians(tx[4])),
+                              np.sin(np.radians(tx[3])) * np.cos(np.radians(tx[4])), np.sin(np.radians(tx[4]))])
+                a = tx[:3] - d * tx[6] / 2
+                pts = np.array([a + d * tx[6] / 20 * (i + 0.5) for i in range(20)])
+            dt = c.find_cell_around_point(pts)
+            sr, si = c.assemble_rhs_csem(fidx, tx, dt)
+            osr, osi = O.rhs_csem(om, f, tx)
+            assert np.abs(sr).max() == 0.0
+            assert np.abs(si - osi).max() <= 1e-12 * np.abs(osi).max()
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
