@@ -103,6 +103,7 @@ _SIGS = {
     "emg_point_index_find": ([_P, _I, _P, _P], _I),
     "emg_point_index_destroy": ([_P], None),
     "emg_find_cell_around_point": ([_P, _I, _P, _P], _I),
+    "emg_interpolate_fields_host": ([_P, _I, _I, _P, _P, _P, _P, _P], _I),
     "emg_survey_read_emd": ([C.c_char_p], _P),
     "emg_survey_sizes": ([_P, _P, _P, _P, _P], _I),
     "emg_survey_get": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
@@ -499,6 +500,15 @@ class EMContext:
         om = _f64(omegas)
         _check(lib().emg_spmv_complex_dev(self._h, om.size, _ptr(om), C.c_void_p(x_ptr), C.c_void_p(y_ptr),
                                           int(conj_out)))
+
+    def interpolate_fields_host(self, fidx, pts, tets, e_re, e_im):
+        """interpolate_fields (src/em_fwd.cc:719-744) from a host solution;
+        returns E, H as (n, 3) complex arrays."""
+        p = _f64(np.asarray(pts).reshape(-1, 3))
+        eh = np.zeros((p.shape[0], 2, 3), dtype=np.complex128)
+        _check(lib().emg_interpolate_fields_host(self._h, int(fidx), p.shape[0], _ptr(p), _ptr(_i32(tets)),
+                                                 _ptr(_f64(e_re)), _ptr(_f64(e_im)), _ptr(eh.view(np.float64))))
+        return eh[:, 0, :], eh[:, 1, :]
 
     def find_cell_around_point(self, pts):
         """find_cell_around_point (src/em_mesh.cc:527-566) on the context's mesh."""

@@ -1332,30 +1332,23 @@ int emg_refine_fixed_number(int n, const double *err, double fraction, unsigned 
 }
 
 // interpolate_fields (src/em_fwd.cc:719-744)
-int emg_interpolate_fields(emg_context *c, int target, int fidx, int n, const double *pts, const int *tets,
-                           double *eh) {
-  EMG_API_BEGIN
-  need(c && pts && tets && eh, EMG_ERR_ARG, "null argument");
-  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
-  use_device(*c);
-  DBuf<double> &x = slot_buf(*c, target);
-  std::vector<double> v((size_t)c->ne * 2);
-  x.download(v.data(), v.size(), c->stream);
-  EMG_CUDA(cudaStreamSynchronize(c->stream));
+// E and H at n points in known cells from an edge solution v (complex,
+// interleaved re/im per edge): interpolate_fields (src/em_fwd.cc:719-744)
+static void interpolate_host(const Context &c, double freq, int n, const double *pts, const int *tets,
+                             const double *v, double *eh) {
   typedef std::complex<double> zc;
-  const double freq = c->freqs[fidx];
   const zc hfac = -1.0 / (zc(0, 1) * 2.0 * PI * freq * MU);
   for (int r = 0; r < n; ++r) {
     int t = tets[r];
-    if (t < 0 || t >= c->nt) fail(EMG_ERR_USER, "Receiver %d is not found in mesh.", r);
+    if (t < 0 || t >= c.nt) fail(EMG_ERR_USER, "Receiver %d is not found in mesh.", r);
     HostTet h;
-    host_tet(*c, t, h);
+    host_tet(c, t, h);
     zc E[3] = {0.0, 0.0, 0.0}, H[3] = {0.0, 0.0, 0.0};
     for (int i = 0; i < 6; ++i) {
       double phi[3];
       int ge;
-      host_phi(*c, h, t, i, pts + 3 * r, phi, &ge);
-      int e = ge, a = c->h_edges[2 * (size_t)e], b = c->h_edges[2 * (size_t)e + 1];
+      host_phi(c, h, t, i, pts + 3 * r, phi, &ge);
+      int e = ge, a = c.h_edges[2 * (size_t)e], b = c.h_edges[2 * (size_t)e + 1];
       int la = 0, lb = 0;
       for (int q = 0; q < 4; ++q) {
         if (h.v[q] == a) la = q;
@@ -1377,6 +1370,34 @@ int emg_interpolate_fields(emg_context *c, int target, int fidx, int n, const do
       eh[12 * r + 6 + 2 * d + 1] = H[d].imag();
     }
   }
+}
+
+int emg_interpolate_fields(emg_context *c, int target, int fidx, int n, const double *pts, const int *tets,
+                           double *eh) {
+  EMG_API_BEGIN
+  need(c && pts && tets && eh, EMG_ERR_ARG, "null argument");
+  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
+  use_device(*c);
+  DBuf<double> &x = slot_buf(*c, target);
+  std::vector<double> v((size_t)c->ne * 2);
+  x.download(v.data(), v.size(), c->stream);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  interpolate_host(*c, c->freqs[fidx], n, pts, tets, v.data(), eh);
+  EMG_API_END
+}
+
+int emg_interpolate_fields_host(emg_context *c, int fidx, int n, const double *pts, const int *tets,
+                                const double *e_re, const double *e_im, double *eh) {
+  EMG_API_BEGIN
+  need(c && pts && tets && e_re && e_im && eh, EMG_ERR_ARG, "null argument");
+  need(c->nt > 0, EMG_ERR_STATE, "interpolate_fields before emg_set_mesh");
+  need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
+  std::vector<double> v((size_t)c->ne * 2);
+  for (int e = 0; e < c->ne; ++e) {
+    v[2 * (size_t)e] = e_re[e];
+    v[2 * (size_t)e + 1] = e_im[e];
+  }
+  interpolate_host(*c, c->freqs[fidx], n, pts, tets, v.data(), eh);
   EMG_API_END
 }
 

@@ -170,6 +170,11 @@ int emg_refine_fixed_number(int n, const double *err, double fraction, unsigned 
  * cells: E and H (6 complex, interleaved re/im) per point from slot target. */
 int emg_interpolate_fields(emg_context *ctx, int target, int fidx, int n, const double *pts,
                            const int *tets, double *eh);
+/* the same from a solution the caller holds on the host (e_re, e_im: one
+ * value per edge, the reference's PETScBlockVector parts); works on a
+ * host-only context */
+int emg_interpolate_fields_host(emg_context *ctx, int fidx, int n, const double *pts, const int *tets,
+                                const double *e_re, const double *e_im, double *eh);
 
 /* find_cell_around_point (src/em_mesh.cc:527-566) for many points: the
  * reference's walk (from the last tet of the closest vertex, breadth-first
