@@ -104,6 +104,7 @@ _SIGS = {
     "emg_point_index_destroy": ([_P], None),
     "emg_find_cell_around_point": ([_P, _I, _P, _P], _I),
     "emg_interpolate_fields_host": ([_P, _I, _I, _P, _P, _P, _P, _P], _I),
+    "emg_save_vtk": ([_P, C.c_char_p, _I, _P, _P], _I),
     "emg_survey_read_emd": ([C.c_char_p], _P),
     "emg_survey_sizes": ([_P, _P, _P, _P, _P], _I),
     "emg_survey_get": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
@@ -509,6 +510,19 @@ class EMContext:
         _check(lib().emg_interpolate_fields_host(self._h, int(fidx), p.shape[0], _ptr(p), _ptr(_i32(tets)),
                                                  _ptr(_f64(e_re)), _ptr(_f64(e_im)), _ptr(eh.view(np.float64))))
         return eh[:, 0, :], eh[:, 1, :]
+
+    def save_vtk(self, path, arrays=None):
+        """Mesh::save_vtk (src/em_mesh.cc:183-248): the mesh with tet_attr and
+        the given per-tet arrays ({name: values}) as legacy ASCII VTK."""
+        arrays = arrays or {}
+        names = (C.c_char_p * max(1, len(arrays)))(*[k.encode() for k in arrays])
+        vals = [_f64(v) for v in arrays.values()]
+        for v in vals:
+            if v.size != self.nt:
+                raise EMGError(EMG_ERR_ARG, "one value per tet")
+        ptrs = (C.c_void_p * max(1, len(vals)))(*[v.ctypes.data for v in vals])
+        _check(lib().emg_save_vtk(self._h, os.fsencode(path), len(vals), C.cast(names, C.c_void_p),
+                                  C.cast(ptrs, C.c_void_p)))
 
     def find_cell_around_point(self, pts):
         """find_cell_around_point (src/em_mesh.cc:527-566) on the context's mesh."""

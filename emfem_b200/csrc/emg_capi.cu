@@ -1225,6 +1225,25 @@ int emg_survey_write_rsp(const emg_survey *h, const char *path, const double *rs
 
 void emg_survey_destroy(emg_survey *h) { delete h; }
 
+int emg_save_vtk(emg_context *c, const char *path, int n_arrays, const char *const *names,
+                 const double *const *data) {
+  EMG_API_BEGIN
+  need(c && path && n_arrays >= 0 && (n_arrays == 0 || (names && data)), EMG_ERR_ARG, "null argument");
+  need(c->nt > 0, EMG_ERR_STATE, "save_vtk before emg_set_mesh");
+  std::vector<std::pair<std::string, const double *>> arrays;
+  for (int k = 0; k < n_arrays; ++k) {
+    need(names[k] && data[k], EMG_ERR_ARG, "null array");
+    const std::string nm = names[k];
+    need(!nm.empty() && nm.find_first_of(" \t\n") == std::string::npos, EMG_ERR_ARG,
+         "array names must be non-empty single words");
+    arrays.push_back({nm, data[k]});
+  }
+  std::string err;
+  if (!emg::write_vtk(path, c->nv, c->h_pts.data(), c->nt, c->h_tets.data(), c->h_attr.data(), arrays, err))
+    fail(EMG_ERR_USER, "%s", err.c_str());
+  EMG_API_END
+}
+
 // calculate_response_mt (em_fwd.cc:747-800): the reference's tensor
 // impedance and tipper formulas per observation, plus apparent resistivity
 // and phase from Z_XY / Z_YX.

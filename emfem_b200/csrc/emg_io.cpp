@@ -14,6 +14,7 @@
 // .rsp: the reference's exact layout and printf formats; AP observations
 // and responses are written back as (exp real, imag in degrees).
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -140,6 +141,61 @@ bool write_rsp(const std::string &path, const Survey &s, const std::complex<doub
       std::fprintf(fp, "% 7d % 6d % 5d % 7d % 13.6E % 13.6E % 13.6E % 13.6E\n", s.otype[i], s.fidx[i], s.tidx[i],
                    s.ridx[i], s.obs[i].real(), s.obs[i].imag(), rsp[i].real(), rsp[i].imag());
     }
+  }
+  const bool ok = std::fclose(fp) == 0;
+  if (!ok) err = "error closing " + path + ".";
+  return ok;
+}
+
+// Mesh::save_vtk (src/em_mesh.cc:183-248): legacy ASCII unstructured grid
+// with the tets, then cell data "subdomain" (0 on one process), "tet_attr"
+// and the caller's arrays in name order (the reference keeps them in a
+// std::map).
+bool write_vtk(const std::string &path, int nv, const double *pts, int nt, const int *tets, const int *attr,
+               const std::vector<std::pair<std::string, const double *>> &arrays, std::string &err) {
+  FILE *fp = std::fopen(path.c_str(), "w");
+  if (!fp) {
+    err = "Unable to open file " + path + " for writing.";
+    return false;
+  }
+  std::fprintf(fp, "# vtk DataFile Version 2.0\n");
+  std::fprintf(fp, "Unstructured Grid\n");
+  std::fprintf(fp, "ASCII\n");
+  std::fprintf(fp, "DATASET UNSTRUCTURED_GRID\n");
+  std::fprintf(fp, "POINTS %d double\n", nv);
+  for (int i = 0; i < nv; ++i)
+    std::fprintf(fp, "%.17g %.17g %.17g\n", pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2]);
+  std::fprintf(fp, "\n");
+  std::fprintf(fp, "CELLS %d %d\n", nt, nt * (4 + 1));
+  for (int i = 0; i < nt; ++i) {
+    std::fprintf(fp, "%d", 4);
+    for (int j = 0; j < 4; ++j) std::fprintf(fp, " %4d", tets[4 * (size_t)i + j]);
+    std::fprintf(fp, "\n");
+  }
+  std::fprintf(fp, "\n");
+  std::fprintf(fp, "CELL_TYPES %d\n", nt);
+  for (int i = 0; i < nt; ++i) std::fprintf(fp, "%d\n", 10);
+  std::fprintf(fp, "\n");
+  std::fprintf(fp, "CELL_DATA %d\n", nt);
+  std::fprintf(fp, "SCALARS subdomain double 1\n");
+  std::fprintf(fp, "LOOKUP_TABLE default\n");
+  for (int i = 0; i < nt; ++i) std::fprintf(fp, "%.15g\n", 0.0);
+  std::fprintf(fp, "\n");
+  std::fprintf(fp, "SCALARS tet_attr double 1\n");
+  std::fprintf(fp, "LOOKUP_TABLE default\n");
+  for (int i = 0; i < nt; ++i) std::fprintf(fp, "%.15g\n", (double)attr[i]);
+  std::fprintf(fp, "\n");
+  std::vector<std::pair<std::string, const double *>> sorted(arrays);
+  std::stable_sort(sorted.begin(), sorted.end(),
+                   [](const std::pair<std::string, const double *> &a, const std::pair<std::string, const double *> &b) {
+                     return a.first < b.first;
+                   });
+  for (size_t k = 0; k < sorted.size(); ++k) {
+    if (k > 0 && sorted[k].first == sorted[k - 1].first) continue;  // a map keeps one array per name
+    std::fprintf(fp, "SCALARS %s double 1\n", sorted[k].first.c_str());
+    std::fprintf(fp, "LOOKUP_TABLE default\n");
+    for (int i = 0; i < nt; ++i) std::fprintf(fp, "%.15g\n", sorted[k].second[i]);
+    std::fprintf(fp, "\n");
   }
   const bool ok = std::fclose(fp) == 0;
   if (!ok) err = "error closing " + path + ".";

@@ -3,6 +3,7 @@
 
 #include <complex>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace emg {
@@ -17,5 +18,7 @@ struct Survey {
 
 bool read_emd(const std::string &path, Survey &s, std::string &err);
 bool write_rsp(const std::string &path, const Survey &s, const std::complex<double> *rsp, std::string &err);
+bool write_vtk(const std::string &path, int nv, const double *pts, int nt, const int *tets, const int *attr,
+               const std::vector<std::pair<std::string, const double *>> &arrays, std::string &err);
 
 }  // namespace emg

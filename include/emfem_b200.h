@@ -251,6 +251,13 @@ int emg_survey_get(const emg_survey *s, double *freqs, double *tx, double *rx, i
 int emg_survey_write_rsp(const emg_survey *s, const char *path, const double *rsp);
 void emg_survey_destroy(emg_survey *s);
 
+/* Mesh::save_vtk (src/em_mesh.cc:183-248): the context's mesh as a legacy
+ * ASCII VTK unstructured grid with cell data "subdomain" (0: one process),
+ * "tet_attr" and n_arrays per-tet arrays (names[k], data[k][nt]) written in
+ * name order; a repeated name keeps its first array.  Host only. */
+int emg_save_vtk(emg_context *ctx, const char *path, int n_arrays, const char *const *names,
+                 const double *const *data);
+
 /* ---- batched fast path (no reference counterpart: replaces the per-task
  * loop of forward_mt/forward_csem, src/em_fwd.cc:1320-1439) -------------
  * Solves k right-hand sides with individual frequencies as one block:

@@ -117,3 +117,29 @@ def test_survey_responses_round_trip(tmp_path):
     rows = [l.split() for l in out.read_text().splitlines()[-2:]]
     assert [float(v) for v in rows[0][4:]] == [100.0, 45.0, 100.0, 45.0]
     assert [float(v) for v in rows[1][4:]] == [100.0, -135.0, 100.0, -135.0]
+
+
+def test_save_vtk_layout(tmp_path):
+    """Mesh::save_vtk (src/em_mesh.cc:183-248) on a host-only context: the
+    text equals the reference's printf formats applied in Python, with the
+    caller's arrays after subdomain and tet_attr in name order."""
+    from emfem_b200 import meshgen as mg
+    prob = mg.mt_halfspace_block(300, freqs=(1.0,), name="vtk")
+    m = prob.mesh
+    rng = np.random.default_rng(4)
+    err_xy, rho = rng.random(m.n_tets), rng.random(m.n_tets) * 100
+    out = tmp_path / "m.vtk"
+    with E.EMContext(-1) as c:
+        c.set_mesh(m)
+        c.save_vtk(str(out), {"rho": rho, "error_xy": err_xy})
+    want = ["# vtk DataFile Version 2.0\n", "Unstructured Grid\n", "ASCII\n", "DATASET UNSTRUCTURED_GRID\n",
+            "POINTS %d double\n" % m.n_vertices]
+    want += ["%.17g %.17g %.17g\n" % tuple(p) for p in m.points]
+    want += ["\n", "CELLS %d %d\n" % (m.n_tets, 5 * m.n_tets)]
+    want += ["%d" % 4 + "".join(" %4d" % v for v in t) + "\n" for t in m.tets]
+    want += ["\n", "CELL_TYPES %d\n" % m.n_tets] + ["10\n"] * m.n_tets + ["\n", "CELL_DATA %d\n" % m.n_tets]
+    for name, vals in (("subdomain", np.zeros(m.n_tets)), ("tet_attr", np.asarray(m.attr, dtype=float)),
+                       ("error_xy", err_xy), ("rho", rho)):
+        want += ["SCALARS %s double 1\n" % name, "LOOKUP_TABLE default\n"]
+        want += ["%.15g\n" % v for v in vals] + ["\n"]
+    assert out.read_text().splitlines(keepends=True) == want
