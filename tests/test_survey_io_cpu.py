@@ -143,3 +143,41 @@ def test_save_vtk_layout(tmp_path):
         want += ["SCALARS %s double 1\n" % name, "LOOKUP_TABLE default\n"]
         want += ["%.15g\n" % v for v in vals] + ["\n"]
     assert out.read_text().splitlines(keepends=True) == want
+
+
+def test_edge_cases_of_the_host_entry_points(tmp_path):
+    """Empty and malformed inputs: zero observations and zero receivers are
+    valid; bad array names, wrong lengths, unwritable paths and calls before
+    a mesh fail with the documented status instead of writing garbage."""
+    p = tmp_path / "empty.emd"
+    p.write_text("0\n0\n0\n0\n")
+    s = E.Survey(str(p))
+    assert s.freqs.size == 0 and s.tx.shape == (0, 7) and s.rx.shape == (0, 3) and s.obs.size == 0
+    s.write_rsp(str(tmp_path / "empty.rsp"), np.zeros(0, dtype=np.complex128))
+    assert (tmp_path / "empty.rsp").read_text().splitlines()[-2:] == ["0", "#%6s %6s %5s %7s %13s %13s %13s %13s" % (
+        "otype", "fidx", "tidx", "ridx", "amp", "phase", "amp`", "phase`")]
+    with pytest.raises(E.EMGError) as ei:
+        s.write_rsp(str(tmp_path / "no_such_dir" / "x.rsp"), np.zeros(0, dtype=np.complex128))
+    assert ei.value.code == E.api.EMG_ERR_USER
+    assert E.calculate_response_mt(1.0, np.zeros((0, 4, 3)), [], []).size == 0
+    with pytest.raises(E.EMGError) as ei:
+        E.calculate_response_mt(0.0, np.ones((1, 4, 3)), [E.api.Z_XY_RI], [0])
+    assert ei.value.code == E.api.EMG_ERR_ARG
+    from emfem_b200 import meshgen as mg
+    prob = mg.mt_halfspace_block(300, freqs=(1.0,), name="edge")
+    with E.EMContext(-1) as c:
+        with pytest.raises(E.EMGError) as ei:
+            c.save_vtk(str(tmp_path / "a.vtk"))
+        assert ei.value.code == E.api.EMG_ERR_STATE
+        with pytest.raises(E.EMGError) as ei:
+            c.find_cell_around_point(np.zeros((1, 3)))
+        assert ei.value.code == E.api.EMG_ERR_STATE
+        c.set_mesh(prob.mesh)
+        with pytest.raises(E.EMGError) as ei:
+            c.save_vtk(str(tmp_path / "a.vtk"), {"two words": np.zeros(prob.mesh.n_tets)})
+        assert ei.value.code == E.api.EMG_ERR_ARG
+        with pytest.raises(E.EMGError):
+            c.save_vtk(str(tmp_path / "a.vtk"), {"short": np.zeros(3)})
+        c.save_vtk(str(tmp_path / "a.vtk"))  # mesh only: subdomain and tet_attr
+        text = (tmp_path / "a.vtk").read_text()
+        assert "SCALARS tet_attr double 1" in text and text.count("SCALARS") == 2
