@@ -532,6 +532,14 @@ int emg_create_context(emg_context **ctx, int device) {
     delete c;
     check_cuda(e, "cudaStreamCreate", __FILE__, __LINE__);
   }
+  try {
+    // the allocation-free estimator's scratch address, looked up now so that
+    // its module is loaded and the address cached before any run
+    (void)noalloc_scratch_address(device);
+  } catch (...) {
+    delete c;
+    throw;
+  }
   *ctx = c;
   EMG_API_END
 }

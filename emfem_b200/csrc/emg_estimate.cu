@@ -384,9 +384,15 @@ constexpr int kNoAllocMaxSol = 3;        // MT: XY, YX and the dual solution
 // held on every GPU that loads the library until the process exits
 __device__ __align__(256) double g_estimate_scratch[kNoAllocMaxSol * kNoAllocMaxTets * 5];
 
+}  // namespace
+
+namespace emg {
 // In host code g_estimate_scratch only names a host-side stand-in; the device
-// address is looked up once per device, with that device current.
-double *scratch_address(int device) {
+// address is looked up once per device, with that device current.  Device
+// contexts call this when they are created, which also loads this file's
+// module on that device, so emg_estimate_error_noalloc itself never loads a
+// module or allocates.
+double *noalloc_scratch_address(int device) {
   static std::mutex mu;
   static std::map<int, double *> addr;
   std::lock_guard<std::mutex> lock(mu);
@@ -398,8 +404,7 @@ double *scratch_address(int device) {
   addr[device] = p;
   return p;
 }
-
-}  // namespace
+}  // namespace emg
 
 extern "C" int emg_estimate_error_noalloc(emg_context *ctx, int fidx, int tidx, double *err_dev, double *eta_dev) {
   using namespace emg;
@@ -422,7 +427,7 @@ extern "C" int emg_estimate_error_noalloc(emg_context *ctx, int fidx, int tidx, 
       sp[s] = it->second.p;
     }
     check_cuda(cudaSetDevice(c.device), "cudaSetDevice", __FILE__, __LINE__);
-    double *scratch = scratch_address(c.device);
+    double *scratch = noalloc_scratch_address(c.device);
     // every volume and face entry is written before it is read, so nothing
     // left in the array by an earlier call needs clearing
     launch_estimate(c, 2 * PI * c.freqs[fidx], nsol, sp, eta_dev, err_dev, scratch, scratch + (size_t)nsol * c.nt);

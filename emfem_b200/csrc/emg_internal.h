@@ -259,6 +259,10 @@ struct Context {
 const TiledPattern *tiled_pattern(Context &c, const int *rp_dev, const std::vector<int> &h_rp,
                                   const std::vector<int> &h_ci, int row_bytes);
 
+// device address of the fixed scratch of emg_estimate_error_noalloc on a
+// device (looked up once per device, with it current; emg_estimate.cu)
+double *noalloc_scratch_address(int device);
+
 // records the message returned by emg_last_error() on this thread
 void set_last_error(const char *msg);
 

@@ -155,10 +155,14 @@ int emg_estimate_error(emg_context *ctx, int fidx, int tidx, double *err, double
  * in a fixed 15.7 MB device array of the library (held on every GPU that
  * loads it), so meshes above 131072 tets are rejected with EMG_ERR_ARG.
  * err_dev (n_err x T) and eta_dev (n_sol x T) are caller-owned device
- * buffers laid out as in emg_estimate_error.  The first call on a device
- * looks up the array's device address; make that call before any stream
- * capture.  Every call shares the array: calls that overlap on the GPU (two
- * contexts or threads at once) race.  Returns after the stream completes. */
+ * buffers laid out as in emg_estimate_error.  The array's device address is
+ * looked up when a device context is created (emg_create_context), so this
+ * call loads no module and allocates nothing.  It runs on the context's own
+ * stream, which is not ordered after the caller's streams: any pending work
+ * of the caller that writes or reads err_dev/eta_dev must be complete before
+ * the call (synchronise that stream first).  Every call shares the array:
+ * calls that overlap on the GPU (two contexts or threads at once) race.
+ * Returns after the context's stream completes, so the outputs are ready. */
 int emg_estimate_error_noalloc(emg_context *ctx, int fidx, int tidx, double *err_dev, double *eta_dev);
 
 /* refine_fixed_fraction / refine_fixed_number (src/em_fwd.cc:1182-1240):

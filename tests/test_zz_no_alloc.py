@@ -51,12 +51,50 @@ def test_noalloc_estimate_matches_allocating_entry_point():
             err_ref, eta_ref = c.estimate_error(fidx, -3)
             err_d.fill_(float("nan"))
             eta_d.fill_(float("nan"))
+            # the entry point runs on the context's stream, which is not
+            # ordered after torch's: the fills must be finished first
+            torch.cuda.synchronize()
             c.estimate_error_noalloc_dev(fidx, -3, err_d.data_ptr(), eta_d.data_ptr())
             err = err_d.cpu().numpy().reshape(2, nt)
             eta = eta_d.cpu().numpy().reshape(3, nt)
             assert np.isfinite(err).all() and np.isfinite(eta).all()
             assert np.abs(eta - eta_ref).max() <= 1e-10 * np.abs(eta_ref).max()
             assert np.abs(err - err_ref).max() <= 1e-10 * np.abs(err_ref).max()
+
+
+def test_noalloc_estimate_csem_matches_allocating_entry_point():
+    """CSEM form: two solutions (source and dual), one indicator per tet."""
+    import torch
+    prob = mg.marine_csem(5000, freqs=(0.25, 1.25), name="noalloc-csem")
+    loc = mg.PointLocator(prob.mesh)
+    tx = prob.survey.tx[0]
+    rx = prob.survey.rx
+    with E.EMContext(0) as c:
+        c.set_mesh(prob.mesh)
+        c.set_model(prob.model)
+        c.set_frequencies(prob.survey.freqs)
+        c.create_linear_system(0)
+        nt = prob.mesh.n_tets
+        err_d = torch.empty(nt, dtype=torch.float64, device="cuda")
+        eta_d = torch.empty(2 * nt, dtype=torch.float64, device="cuda")
+        for fidx in (0, 1):
+            c.assemble_matrix(fidx)
+            c.create_pc()
+            sr, si = c.assemble_rhs_csem(fidx, tx, loc.locate_all(tx[None, :3]))
+            c.solve_linear_system(E.SOL_CSEM, sr, si, 100, 1e-8)
+            sr, si = c.assemble_rhs_dual(rx, loc.locate_all(rx))
+            c.solve_linear_system(E.SOL_DUAL, sr, si, 100, 1e-6)
+            for _ in range(2):
+                err_ref, eta_ref = c.estimate_error(fidx, 0)
+                err_d.fill_(float("nan"))
+                eta_d.fill_(float("nan"))
+                torch.cuda.synchronize()
+                c.estimate_error_noalloc_dev(fidx, 0, err_d.data_ptr(), eta_d.data_ptr())
+                err = err_d.cpu().numpy().reshape(1, nt)
+                eta = eta_d.cpu().numpy().reshape(2, nt)
+                assert np.isfinite(err).all() and np.isfinite(eta).all()
+                assert np.abs(eta - eta_ref).max() <= 1e-10 * np.abs(eta_ref).max()
+                assert np.abs(err - err_ref).max() <= 1e-10 * np.abs(err_ref).max()
 
 
 def test_noalloc_estimate_rejects_meshes_beyond_its_scratch():
