@@ -105,6 +105,9 @@ _SIGS = {
     "emg_find_cell_around_point": ([_P, _I, _P, _P], _I),
     "emg_interpolate_fields_host": ([_P, _I, _I, _P, _P, _P, _P, _P], _I),
     "emg_save_vtk": ([_P, C.c_char_p, _I, _P, _P], _I),
+    "emg_interpolate_fields_block_dev": ([_P, _I, _P, _P, _I, _P, _P, _P], _I),
+    "emg_assemble_rhs_csem_block_dev": ([_P, _I, _P, _P, _P], _I),
+    "emg_assemble_rhs_dual_block_dev": ([_P, _I, _I, _P, _P], _I),
     "emg_survey_read_emd": ([C.c_char_p], _P),
     "emg_survey_sizes": ([_P, _P, _P, _P, _P], _I),
     "emg_survey_get": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
@@ -496,6 +499,29 @@ class EMContext:
         _check(lib().emg_solve_block_dev(self._h, k, _ptr(freqs), C.c_void_p(rhs_ptr), C.c_void_p(x_ptr),
                                          C.byref(o), C.cast(infos, C.c_void_p)))
         return list(infos)
+
+    def interpolate_fields_block_dev(self, freqs, x_ptr, pts, tets):
+        """E and H of every column of a device block (n_edges x k complex) at
+        receivers with known cells; returns E, H as (n_rx, k, 3) complex."""
+        freqs = _f64(freqs)
+        k = freqs.size
+        p = _f64(np.asarray(pts).reshape(-1, 3))
+        eh = np.zeros((p.shape[0], k, 2, 3), dtype=np.complex128)
+        _check(lib().emg_interpolate_fields_block_dev(self._h, k, _ptr(freqs), C.c_void_p(x_ptr), p.shape[0],
+                                                      _ptr(p), _ptr(_i32(tets)), _ptr(eh.view(np.float64))))
+        return eh[:, :, 0, :], eh[:, :, 1, :]
+
+    def assemble_rhs_csem_block_dev(self, freqs, tx, s_ptr):
+        """CSEM right-hand sides for k (transmitter, frequency) columns into a
+        device block; tx: (k, 7)."""
+        freqs = _f64(freqs)
+        t = _f64(np.asarray(tx).reshape(freqs.size, 7))
+        _check(lib().emg_assemble_rhs_csem_block_dev(self._h, freqs.size, _ptr(freqs), _ptr(t), C.c_void_p(s_ptr)))
+
+    def assemble_rhs_dual_block_dev(self, k, rx, s_ptr):
+        """The dual right-hand side in all k columns of a device block."""
+        r = _f64(np.asarray(rx).reshape(-1, 3))
+        _check(lib().emg_assemble_rhs_dual_block_dev(self._h, int(k), r.shape[0], _ptr(r), C.c_void_p(s_ptr)))
 
     def spmv_complex_dev(self, omegas, x_ptr, y_ptr, conj_out=False):
         om = _f64(omegas)

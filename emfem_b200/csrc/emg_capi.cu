@@ -112,6 +112,7 @@ struct Workspace {
   DBuf<float> f_in, f_out;         // FP32 inner vectors
   DBuf<double> est_vol, est_fe, est_eta, est_err;
   DBuf<double> bvals, omega_k, omega_cols;
+  DBuf<double> blk_rhs, blk_x;     // one padded block of a wider or ragged solve
   // plain path: hierarchy of B(w) for the assembled frequency (create_pc)
   Ams<double> pams64;
   // batched path: two-part hierarchy valid for every frequency of a block
@@ -506,6 +507,38 @@ static std::vector<double> interleave(const double *re, const double *im, int n)
 }  // namespace emg
 
 using namespace emg;
+
+// Eigen::VectorXd::sum() (the total of refine_fixed_fraction,
+// src/em_fwd.cc:1192) in the order Eigen evaluates it when the reference is
+// built for x86-64 without -march flags, where Eigen vectorises with SSE2
+// packets of two doubles: two packet accumulators advance over pairs of
+// packets, then they are added, a leftover whole packet is added, the two
+// lanes are summed, and an odd last element comes last.  The threshold, and
+// so the flag set, can move by one ulp of the total with another order.
+static double eigen_sse2_sum(const double *x, int n) {
+  if (n < 2) return n == 1 ? x[0] : 0.0;
+  const int n1 = n / 2 * 2;  // elements in whole packets
+  const int n2 = n / 4 * 4;  // elements in whole packet pairs
+  double a0 = x[0], a1 = x[1];
+  if (n1 > 2) {
+    double b0 = x[2], b1 = x[3];
+    for (int i = 4; i < n2; i += 4) {
+      a0 += x[i];
+      a1 += x[i + 1];
+      b0 += x[i + 2];
+      b1 += x[i + 3];
+    }
+    a0 += b0;
+    a1 += b1;
+    if (n1 > n2) {
+      a0 += x[n2];
+      a1 += x[n2 + 1];
+    }
+  }
+  double r = a0 + a1;
+  for (int i = n1; i < n; ++i) r += x[i];
+  return r;
+}
 
 extern "C" {
 
@@ -1105,8 +1138,7 @@ int emg_estimate_error(emg_context *c, int fidx, int tidx, double *err, double *
 int emg_refine_fixed_fraction(int n, const double *err, double fraction, unsigned char *flag) {
   EMG_API_BEGIN
   need(n >= 0 && (n == 0 || (err && flag)), EMG_ERR_ARG, "null argument");
-  double total = 0;
-  for (int i = 0; i < n; ++i) total += err[i];
+  const double total = eigen_sse2_sum(err, n);
   std::vector<double> s(err, err + n);
   std::sort(s.begin(), s.end(), std::greater<double>());
   double sum = 0, thr = 0;
@@ -1181,10 +1213,11 @@ int emg_interpolate_fields(emg_context *c, int target, int fidx, int n, const do
   need(fidx >= 0 && fidx < (int)c->freqs.size(), EMG_ERR_ARG, "frequency index out of range");
   use_device(*c);
   DBuf<double> &x = slot_buf(*c, target);
-  std::vector<double> v((size_t)c->ne * 2);
-  x.download(v.data(), v.size(), c->stream);
-  EMG_CUDA(cudaStreamSynchronize(c->stream));
-  interpolate_host(*c, c->freqs[fidx], n, pts, tets, v.data(), eh);
+  // the slot is an n x 1 complex block: the receiver kernel reads only the
+  // edges of the receivers' cells
+  const double f = c->freqs[fidx];
+  int rc = emg_interpolate_fields_block_dev(c, 1, &f, x.p, n, pts, tets, eh);
+  if (rc != EMG_OK) fail(rc, "%s", emg_last_error());
   EMG_API_END
 }
 
@@ -1211,9 +1244,10 @@ __global__ static void conj_copy_kernel(long n, const double2 *a, double2 *b) {
   }
 }
 
-// batched fast path on device vectors
-static void solve_block_dev(Context &c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
-                            const emg_block_opts &o, emg_solve_info *infos) {
+// batched fast path on device vectors, one block of k (a power of two <= 32)
+// columns
+static void solve_block_pow2(Context &c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                             const emg_block_opts &o, emg_solve_info *infos) {
   need(c.assembled, EMG_ERR_STATE, "solve_block before assemble_matrix");
   need(k >= 1 && (k & (k - 1)) == 0 && k <= 32, EMG_ERR_ARG, "block width k must be a power of two <= 32");
   Workspace &w = *c.ws;
@@ -1323,6 +1357,52 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
   if (infos)
     for (int j = 0; j < k; ++j) fill_info(&infos[j], st, inner, j);
   c.kernel_ms["solve_block"] = st.seconds * 1e3;
+}
+
+// Any number of columns: blocks of at most kMaxBlock columns solved one after
+// another; a block whose width is not a power of two is padded with zero
+// right-hand sides (they converge at once and stay inactive in the inner
+// solves) at its last column's frequency.
+static void solve_block_dev(Context &c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                            const emg_block_opts &o, emg_solve_info *infos) {
+  constexpr int kMaxBlock = 32;
+  need(k >= 1, EMG_ERR_ARG, "block width k must be positive");
+  int kp = 1;
+  while (kp < k) kp <<= 1;
+  if (k <= kMaxBlock && kp == k) {
+    solve_block_pow2(c, k, freqs, rhs_dev, x_dev, o, infos);
+    return;
+  }
+  Workspace &w = *c.ws;
+  const size_t n = (size_t)c.ne;
+  double total_s = 0;
+  for (int j0 = 0; j0 < k; j0 += kMaxBlock) {
+    const int kc = std::min(kMaxBlock, k - j0);
+    int kb = 1;
+    while (kb < kc) kb <<= 1;
+    std::vector<double> f(kb, freqs[j0 + kc - 1]);
+    std::copy(freqs + j0, freqs + j0 + kc, f.begin());
+    w.blk_rhs.alloc(n * kb * 2);
+    w.blk_x.alloc(n * kb * 2);
+    const size_t dst_pitch = (size_t)kb * 16, src_pitch = (size_t)k * 16, width = (size_t)kc * 16;
+    if (kb != kc) w.blk_rhs.zero(c.stream);
+    EMG_CUDA(cudaMemcpy2DAsync(w.blk_rhs.p, dst_pitch, rhs_dev + (size_t)j0 * 2, src_pitch, width, n,
+                               cudaMemcpyDeviceToDevice, c.stream));
+    if (o.use_guess) {
+      if (kb != kc) w.blk_x.zero(c.stream);
+      EMG_CUDA(cudaMemcpy2DAsync(w.blk_x.p, dst_pitch, x_dev + (size_t)j0 * 2, src_pitch, width, n,
+                                 cudaMemcpyDeviceToDevice, c.stream));
+    }
+    std::vector<emg_solve_info> inf(kb);
+    solve_block_pow2(c, kb, f.data(), w.blk_rhs.p, w.blk_x.p, o, inf.data());
+    EMG_CUDA(cudaMemcpy2DAsync(x_dev + (size_t)j0 * 2, src_pitch, w.blk_x.p, dst_pitch, width, n,
+                               cudaMemcpyDeviceToDevice, c.stream));
+    total_s += c.kernel_ms["solve_block"] * 1e-3;
+    if (infos)
+      for (int j = 0; j < kc; ++j) infos[j0 + j] = inf[j];
+  }
+  EMG_CUDA(cudaStreamSynchronize(c.stream));
+  c.kernel_ms["solve_block"] = total_s * 1e3;
 }
 
 int emg_solve_block_dev(emg_context *c, int k, const double *freqs, const double *rhs_dev, double *x_dev,

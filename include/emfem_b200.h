@@ -264,7 +264,9 @@ int emg_save_vtk(emg_context *ctx, const char *path, int n_arrays, const char *c
 
 /* ---- batched fast path (no reference counterpart: replaces the per-task
  * loop of forward_mt/forward_csem, src/em_fwd.cc:1320-1439) -------------
- * Solves k right-hand sides with individual frequencies as one block:
+ * Solves k right-hand sides with individual frequencies as blocks of at most
+ * 32 columns, one after another (a block whose width is not a power of two is
+ * padded with zero columns):
  * complex FGMRES (FP64 outer, true residual in FP64) around an AMS-
  * preconditioned FCG whose precision is set by -emg_inner_precision
  * (fp32|fp64).  One AMS hierarchy serves every frequency.
@@ -283,6 +285,27 @@ int emg_solve_block(emg_context *ctx, int k, const double *freqs, const double *
                     const emg_block_opts *opts, emg_solve_info *infos);
 int emg_solve_block_dev(emg_context *ctx, int k, const double *freqs, const double *rhs_dev, double *x_dev,
                         const emg_block_opts *opts, emg_solve_info *infos);
+
+/* interpolate_fields (src/em_fwd.cc:719-744) for a device block x_dev (n_edges
+ * x k complex, interleaved, as emg_solve_block_dev returns it) at n receivers
+ * with known cells: eh[(r*k + j)*12 ...] holds E then H of column j at
+ * receiver r (complex, interleaved re/im), H = -curl E / (i w_j mu).  One
+ * device thread per (receiver, column); only the n x k x 12 values are
+ * copied to the host.  emg_interpolate_fields uses it on a named slot. */
+int emg_interpolate_fields_block_dev(emg_context *ctx, int k, const double *freqs, const double *x_dev, int n,
+                                     const double *pts, const int *tets, double *eh);
+
+/* assemble_rhs_csem (src/em_fwd.cc:582-671) for k columns at once: column j
+ * is transmitter tx[7j .. 7j+7) (TX_SIZE values, line sources divided into
+ * -n_tx_divisions dipoles) at frequency freqs[j].  The host divides the
+ * sources and locates their cells (the reference's walk); the basis values
+ * are evaluated and scattered into the zeroed device block s_dev (n_edges x k
+ * complex) by a kernel.  A dipole outside the mesh: EMG_ERR_USER. */
+int emg_assemble_rhs_csem_block_dev(emg_context *ctx, int k, const double *freqs, const double *tx,
+                                    double *s_dev);
+/* assemble_rhs_dual (src/em_fwd.cc:673-717) into every one of k columns of
+ * s_dev (the dual right-hand side does not depend on the frequency). */
+int emg_assemble_rhs_dual_block_dev(emg_context *ctx, int k, int n_rx, const double *rx, double *s_dev);
 
 /* Batched MT right-hand sides (assemble_rhs_mt, src/em_fwd.cc:488-580, for k
  * columns at once): column j is polarisation modes[j] (EMG_SOL_MT_XY/YX) at

@@ -1498,10 +1498,42 @@ void orc_estimate(const OrcMesh *m, const OrcModel *md, double freq, int nsol, c
   }
 }
 
+
+// Eigen::VectorXd::sum() (the total of refine_fixed_fraction,
+// src/em_fwd.cc:1192) in the order Eigen evaluates it when the reference is
+// built for x86-64 without -march flags, where Eigen vectorises with SSE2
+// packets of two doubles: two packet accumulators advance over pairs of
+// packets, then they are added, a leftover whole packet is added, the two
+// lanes are summed, and an odd last element comes last.  The threshold, and
+// so the flag set, can move by one ulp of the total with another order.
+static double orc_eigen_sse2_sum(const double *x, int n) {
+  if (n < 2) return n == 1 ? x[0] : 0.0;
+  const int n1 = n / 2 * 2;  // elements in whole packets
+  const int n2 = n / 4 * 4;  // elements in whole packet pairs
+  double a0 = x[0], a1 = x[1];
+  if (n1 > 2) {
+    double b0 = x[2], b1 = x[3];
+    for (int i = 4; i < n2; i += 4) {
+      a0 += x[i];
+      a1 += x[i + 1];
+      b0 += x[i + 2];
+      b1 += x[i + 3];
+    }
+    a0 += b0;
+    a1 += b1;
+    if (n1 > n2) {
+      a0 += x[n2];
+      a1 += x[n2 + 1];
+    }
+  }
+  double r = a0 + a1;
+  for (int i = n1; i < n; ++i) r += x[i];
+  return r;
+}
+
 // refine_fixed_fraction (em_fwd.cc:1182-1215)
 void orc_refine_fixed_fraction(int n, const double *err, double fraction, unsigned char *flag) {
-  double total = 0;
-  for (int i = 0; i < n; ++i) total += err[i];
+  const double total = orc_eigen_sse2_sum(err, n);
   std::vector<double> s(err, err + n);
   std::sort(s.begin(), s.end(), std::greater<double>());
   double sum = 0, thr = 0;

@@ -1,0 +1,240 @@
+"""Accuracy of the benchmarked path at the north-star bar, on full-size
+configurations 0 and 1 (seeded synthetic meshes of their shapes and sizes).
+
+The path is emg_solve_block exactly as bench.py runs it: FP64 outer FGMRES to
+a relative residual of 1e-8 (the metric's setting), inner FCG capped at 30
+iterations with truncation 2, FP32 AMS with cycle "0201" (the defaults of the
+batched path).  Right-hand sides come from the device block kernels.
+
+Bars (written per assertion):
+  * receiver E and H within 1e-6 relative of the exact discrete solution
+    (sparse direct FP64 solve), per receiver: max component error over the
+    largest component of the exact field;
+  * MT apparent resistivity within 0.1 % and phase within 0.05 degrees of the
+    exact solution's (calculate_response_mt's AP pair from Z_xy and Z_yx,
+    src/em_fwd.cc:746-802);
+  * error indicators within 1e-8 relative of the oracle's (
+    the largest indicator sets the scale) on the same solutions, and the
+    identical refined-tet set;
+  * the block receiver kernel and the block CSEM/dual right-hand-side kernels
+    against their host restatements to 1e-12.
+"""
+
+import numpy as np
+import pytest
+
+import emfem_b200 as E
+from emfem_b200 import meshgen as mg
+import oracle as O
+from exact_solve import exact_solutions
+
+pytestmark = pytest.mark.gpu
+
+BENCH = dict(rtol=1e-8, max_it=200, inner_fp32=True)
+
+
+def _ctx(prob, tidx):
+    c = E.EMContext(0)
+    c.set_mesh(prob.mesh)
+    c.set_model(prob.model)
+    c.set_frequencies(prob.survey.freqs)
+    c.create_linear_system(tidx)
+    return c
+
+
+def _rel_rows(a, b):
+    """per row: max |a - b| over the largest |b| of that row"""
+    return np.abs(a - b).max(axis=-1) / np.maximum(np.abs(b).max(axis=-1), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def cfg0():
+    import torch
+    prob = mg.config(0)
+    m = prob.mesh
+    freqs = np.asarray(prob.survey.freqs)
+    colf = np.repeat(freqs, 2)
+    modes = np.tile(np.array([E.XY_POLAR, E.YX_POLAR], dtype=np.int32), freqs.size)
+    k = colf.size
+    rx = prob.survey.rx
+    tets = mg.PointLocator(m).locate_all(rx)
+    assert (tets >= 0).all()
+    om = O.Mesh(m)
+    orp, oci = O.sparsity(om)
+    with _ctx(prob, -3) as c:
+        c.set_background(*mg.background_model(m, prob.model))
+        c.assemble_matrix(0)
+        s = torch.zeros((m.n_edges, k), dtype=torch.complex128, device="cuda")
+        x = torch.zeros_like(s)
+        c.assemble_rhs_mt_block_dev(colf, modes, s.data_ptr())
+        infos = c.solve_block_dev(colf, s.data_ptr(), x.data_ptr(), **BENCH)
+        Eb, Hb = c.interpolate_fields_block_dev(colf, x.data_ptr(), rx, tets)
+        xs = x.cpu().numpy()
+        ss = s.cpu().numpy()
+        # receiver kernel against the host restatement on the same solution
+        Eh, Hh = [], []
+        for j in range(k):
+            fidx = int(np.searchsorted(freqs, colf[j]))
+            e_, h_ = c.interpolate_fields_host(fidx, rx, tets, xs[:, j].real, xs[:, j].imag)
+            Eh.append(e_)
+            Hh.append(h_)
+        jobs = []
+        for fi, f in enumerate(freqs):
+            Co, Mo, _ = O.assemble(om, prob.model, f, orp, oci)
+            jobs.append((orp, oci, Co, Mo, np.conj(ss[:, 2 * fi:2 * fi + 2])))
+        z = np.concatenate(exact_solutions(jobs), axis=1)
+        Ez, Hz = [], []
+        for j in range(k):
+            fidx = int(np.searchsorted(freqs, colf[j]))
+            e_, h_ = c.interpolate_fields_host(fidx, rx, tets, z[:, j].real, z[:, j].imag)
+            Ez.append(e_)
+            Hz.append(h_)
+    return dict(prob=prob, freqs=freqs, colf=colf, infos=infos, x=xs, z=z, Eb=Eb, Hb=Hb,
+                Eh=np.stack(Eh, axis=1), Hh=np.stack(Hh, axis=1), Ez=np.stack(Ez, axis=1),
+                Hz=np.stack(Hz, axis=1))
+
+
+def test_cfg0_block_solve_converges(cfg0):
+    assert cfg0["prob"].mesh.n_tets >= 45_000
+    for inf in cfg0["infos"]:
+        assert inf.reason == 0 and inf.true_rel_res <= 1e-8
+
+
+def test_cfg0_receiver_kernel_matches_host(cfg0):
+    assert _rel_rows(cfg0["Eb"], cfg0["Eh"]).max() <= 1e-12
+    assert _rel_rows(cfg0["Hb"], cfg0["Hh"]).max() <= 1e-12
+
+
+def test_cfg0_fields_within_1e6_of_exact(cfg0):
+    x, z = cfg0["x"], cfg0["z"]
+    for j in range(x.shape[1]):
+        assert np.abs(x[:, j] - z[:, j]).max() / np.abs(z[:, j]).max() < 1e-6
+    eE = _rel_rows(cfg0["Eb"], cfg0["Ez"])
+    eH = _rel_rows(cfg0["Hb"], cfg0["Hz"])
+    print("cfg0 receiver error vs exact: E %.2e H %.2e" % (eE.max(), eH.max()))
+    assert eE.max() <= 1e-6
+    assert eH.max() <= 1e-6
+
+
+def _mt_ap(freq, E_, H_, jxy, jyx):
+    nrx = E_.shape[0]
+    fields = np.stack([E_[:, jxy], H_[:, jxy], E_[:, jyx], H_[:, jyx]], axis=1)
+    otype = np.array([E.api.R_XY_AP, E.api.R_YX_AP] * nrx, dtype=np.int32)
+    ridx = np.repeat(np.arange(nrx, dtype=np.int32), 2)
+    return E.calculate_response_mt(freq, fields, otype, ridx)
+
+
+def test_cfg0_mt_rho_a_and_phase(cfg0):
+    worst_rho, worst_ph = 0.0, 0.0
+    for fi, f in enumerate(cfg0["freqs"]):
+        a = _mt_ap(f, cfg0["Eb"], cfg0["Hb"], 2 * fi, 2 * fi + 1)
+        b = _mt_ap(f, cfg0["Ez"], cfg0["Hz"], 2 * fi, 2 * fi + 1)
+        drho = np.abs(np.expm1(a.real - b.real))
+        dph = np.abs(np.degrees(np.angle(np.exp(1j * (a.imag - b.imag)))))
+        worst_rho, worst_ph = max(worst_rho, drho.max()), max(worst_ph, dph.max())
+    print("cfg0 rho_a rel error %.2e, phase error %.2e deg" % (worst_rho, worst_ph))
+    assert worst_rho <= 1e-3
+    assert worst_ph <= 0.05
+
+
+@pytest.fixture(scope="module")
+def cfg1():
+    import torch
+    prob = mg.config(1)
+    m = prob.mesh
+    freqs = np.asarray(prob.survey.freqs)
+    k = freqs.size
+    tx = np.repeat(prob.survey.tx[:1], k, axis=0)
+    rx = prob.survey.rx
+    om = O.Mesh(m)
+    loc = mg.PointLocator(m)
+    out = dict(prob=prob, freqs=freqs)
+    with _ctx(prob, 0) as c:
+        c.assemble_matrix(0)
+        s = torch.zeros((m.n_edges, k), dtype=torch.complex128, device="cuda")
+        d = torch.zeros_like(s)
+        x = torch.zeros_like(s)
+        xd = torch.zeros_like(s)
+        c.assemble_rhs_csem_block_dev(freqs, tx, s.data_ptr())
+        c.assemble_rhs_dual_block_dev(k, rx, d.data_ptr())
+        ss, dd = s.cpu().numpy(), d.cpu().numpy()
+        tx_tets = loc.locate_all(tx[0, None, :3])
+        rx_tets = loc.locate_all(rx)
+        out["rhs_err"] = []
+        for j in range(k):
+            sr, si = c.assemble_rhs_csem(j, tx[j], tx_tets)
+            out["rhs_err"].append(np.abs(ss[:, j] - (sr + 1j * si)).max() / np.abs(si).max())
+        sr, si = c.assemble_rhs_dual(rx, rx_tets)
+        out["dual_err"] = max(np.abs(dd[:, j] - (sr + 1j * si)).max() / np.abs(sr).max() for j in range(k))
+        out["infos"] = c.solve_block_dev(freqs, s.data_ptr(), x.data_ptr(), **BENCH)
+        out["dinfos"] = c.solve_block_dev(freqs, d.data_ptr(), xd.data_ptr(), rtol=1e-6, max_it=200,
+                                          inner_fp32=True)
+        xs, xds = x.cpu().numpy(), xd.cpu().numpy()
+        # GPU estimator on the block solutions, oracle estimator on the same
+        err_b, eta_b, eta_o = [], [], []
+        for j in range(k):
+            c.set_solution(E.SOL_CSEM, xs[:, j].real, xs[:, j].imag)
+            c.set_solution(E.SOL_DUAL, xds[:, j].real, xds[:, j].imag)
+            e_, h_ = c.estimate_error(j, 0)
+            err_b.append(e_[0])
+            eta_b.append(h_)
+            eta_o.append(O.estimate(om, prob.model, freqs[j],
+                                    [(xs[:, j].real, xs[:, j].imag), (xds[:, j].real, xds[:, j].imag)]))
+        # the reference-facing FP64 path at a tight tolerance on the same systems
+        err_p, E_p, E_b = [], [], []
+        for j in range(k):
+            c.assemble_matrix(j)
+            c.create_pc()
+            c.solve_linear_system(E.SOL_CSEM, ss[:, j].real, ss[:, j].imag, 300, 1e-10)
+            c.solve_linear_system(E.SOL_DUAL, dd[:, j].real, dd[:, j].imag, 300, 1e-10)
+            err_p.append(c.estimate_error(j, 0)[0][0])
+            E_p.append(c.interpolate_fields(E.SOL_CSEM, j, rx, rx_tets)[0])
+        E_b = c.interpolate_fields_block_dev(freqs, x.data_ptr(), rx, rx_tets)[0]
+    out.update(err_b=err_b, eta_b=eta_b, eta_o=eta_o, err_p=err_p, E_p=np.stack(E_p, axis=1), E_b=E_b)
+    return out
+
+
+def test_cfg1_block_rhs_kernels_match_host(cfg1):
+    assert cfg1["prob"].mesh.n_tets >= 70_000
+    assert max(cfg1["rhs_err"]) <= 1e-12
+    assert cfg1["dual_err"] <= 1e-12
+
+
+def test_cfg1_solves_converge(cfg1):
+    for inf in cfg1["infos"]:
+        assert inf.reason == 0 and inf.true_rel_res <= 1e-8
+    for inf in cfg1["dinfos"]:
+        assert inf.reason == 0 and inf.true_rel_res <= 1e-6
+
+
+def test_cfg1_csem_fields_within_1e6_of_fp64(cfg1):
+    e = _rel_rows(cfg1["E_b"], cfg1["E_p"])
+    print("cfg1 receiver E error vs FP64 (rtol 1e-10): %.2e" % e.max())
+    assert e.max() <= 1e-6
+
+
+def test_cfg1_estimator_matches_oracle_and_flags_identical(cfg1):
+    worst = 0.0
+    for j in range(len(cfg1["freqs"])):
+        eta_b, eta_o = cfg1["eta_b"][j], cfg1["eta_o"][j]
+        for s in range(2):
+            worst = max(worst, np.abs(eta_b[s] - eta_o[s]).max() / np.abs(eta_o[s]).max())
+        err_o = np.sqrt(eta_o[0] * eta_o[1])
+        assert np.abs(cfg1["err_b"][j] - err_o).max() <= 1e-8 * np.abs(err_o).max()
+        for frac in (0.1, 0.3):
+            assert np.array_equal(E.refine_fixed_fraction(cfg1["err_b"][j], frac),
+                                  O.refine_fixed_fraction(err_o, frac))
+            assert np.array_equal(E.refine_fixed_number(cfg1["err_b"][j], frac),
+                                  O.refine_fixed_number(err_o, frac))
+    print("cfg1 estimator vs oracle: %.2e" % worst)
+    assert worst <= 1e-8
+
+
+def test_cfg1_refined_set_same_as_fp64_solve(cfg1):
+    """The block path (FP32 AMS, rtol 1e-8) marks the same tets as the FP64
+    reference-facing path solved to 1e-10."""
+    for j in range(len(cfg1["freqs"])):
+        a, b = cfg1["err_b"][j], cfg1["err_p"][j]
+        print("cfg1 f=%g indicator difference block vs FP64: %.2e" % (cfg1["freqs"][j],
+                                                                      np.abs(a - b).max() / np.abs(b).max()))
+        assert np.array_equal(E.refine_fixed_fraction(a, 0.1), E.refine_fixed_fraction(b, 0.1))
