@@ -49,6 +49,10 @@ class BlockOpts(C.Structure):
                 ("inner_fp32", C.c_int), ("restart", C.c_int)]
 
 
+class WarmOpts(C.Structure):
+    _fields_ = [("steps", C.c_int), ("batch", C.c_long), ("lr", C.c_float), ("seed", C.c_uint)]
+
+
 def library_path() -> str:
     return os.path.join(_HERE, "libemfem_b200.so")
 
@@ -106,6 +110,12 @@ _SIGS = {
     "emg_interpolate_fields_host": ([_P, _I, _I, _P, _P, _P, _P, _P], _I),
     "emg_save_vtk": ([_P, C.c_char_p, _I, _P, _P], _I),
     "emg_interpolate_fields_block_dev": ([_P, _I, _P, _P, _I, _P, _P, _P], _I),
+    "emg_last_initial_residuals": ([_P, _I, _P], _I),
+    "emg_warm_start_train": ([_P, _I, _P, _P, _P, _P, C.POINTER(WarmOpts), C.POINTER(_D)], _I),
+    "emg_warm_start_predict": ([_P, _I, _P, _P, _P, _P, _I, _P, _P, _P, _I, _P], _I),
+    "emg_warm_start_params": ([_P, _P, _P, C.POINTER(_I)], _I),
+    "emg_warm_start_gradients": ([_P, _I, _P, _P, _P, _P, C.c_long, _I, _P, C.POINTER(_D)], _I),
+    "emg_warm_start_reset": ([_P], _I),
     "emg_assemble_rhs_csem_block_dev": ([_P, _I, _P, _P, _P], _I),
     "emg_assemble_rhs_dual_block_dev": ([_P, _I, _I, _P, _P], _I),
     "emg_survey_read_emd": ([C.c_char_p], _P),
@@ -522,6 +532,59 @@ class EMContext:
         """The dual right-hand side in all k columns of a device block."""
         r = _f64(np.asarray(rx).reshape(-1, 3))
         _check(lib().emg_assemble_rhs_dual_block_dev(self._h, int(k), r.shape[0], _ptr(r), C.c_void_p(s_ptr)))
+
+    def last_initial_residuals(self, k):
+        out = np.zeros(int(k))
+        _check(lib().emg_last_initial_residuals(self._h, int(k), _ptr(out)))
+        return out
+
+    # -- learned warm start ----------------------------------------------------------------
+    @staticmethod
+    def _cols(freqs, src, pos):
+        f = _f64(freqs)
+        s = _i32(src if src is not None else np.zeros(f.size, dtype=np.int32))
+        p = None if pos is None else _f64(np.asarray(pos).reshape(f.size, 3))
+        return f, s, p
+
+    def warm_start_train(self, freqs, src, x_ptr, src_pos=None, steps=300, batch=65536, lr=2e-3, seed=1):
+        """Trains the warm-start network on a solved device block; returns
+        the last minibatch loss."""
+        f, s, p = self._cols(freqs, src, src_pos)
+        o = WarmOpts(int(steps), int(batch), float(lr), int(seed))
+        loss = C.c_double()
+        _check(lib().emg_warm_start_train(self._h, f.size, _ptr(f), _ptr(s), None if p is None else _ptr(p),
+                                          C.c_void_p(x_ptr), C.byref(o), C.byref(loss)))
+        return loss.value
+
+    def warm_start_predict(self, freqs, src, x_ptr, tfreqs, tsrc, guess_ptr, src_pos=None, tsrc_pos=None,
+                           network=True):
+        f, s, p = self._cols(freqs, src, src_pos)
+        tf, ts, tp = self._cols(tfreqs, tsrc, tsrc_pos)
+        _check(lib().emg_warm_start_predict(self._h, f.size, _ptr(f), _ptr(s), None if p is None else _ptr(p),
+                                            C.c_void_p(x_ptr), tf.size, _ptr(tf), _ptr(ts),
+                                            None if tp is None else _ptr(tp), int(bool(network)),
+                                            C.c_void_p(guess_ptr)))
+
+    def warm_start_params(self, set_to=None):
+        n = C.c_int()
+        _check(lib().emg_warm_start_params(self._h, None, None, C.byref(n)))
+        out = np.zeros(n.value, dtype=np.float32)
+        st = None if set_to is None else np.ascontiguousarray(set_to, dtype=np.float32)
+        _check(lib().emg_warm_start_params(self._h, _ptr(out), None if st is None else _ptr(st), None))
+        return out
+
+    def warm_start_gradients(self, freqs, src, x_ptr, batch, step, src_pos=None):
+        f, s, p = self._cols(freqs, src, src_pos)
+        n = C.c_int()
+        _check(lib().emg_warm_start_params(self._h, None, None, C.byref(n)))
+        g = np.zeros(n.value, dtype=np.float32)
+        loss = C.c_double()
+        _check(lib().emg_warm_start_gradients(self._h, f.size, _ptr(f), _ptr(s), None if p is None else _ptr(p),
+                                              C.c_void_p(x_ptr), int(batch), int(step), _ptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def warm_start_reset(self):
+        _check(lib().emg_warm_start_reset(self._h))
 
     def spmv_complex_dev(self, omegas, x_ptr, y_ptr, conj_out=False):
         om = _f64(omegas)

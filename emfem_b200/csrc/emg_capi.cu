@@ -226,6 +226,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_block_inner_rtol") o.block_inner_rtol = getr(k, v);
     else if (key == "emg_block_inner_max_it") o.block_inner_max_it = geti(k, v);
     else if (key == "emg_block_fcg_mmax") o.block_fcg_mmax = geti(k, v);
+    else if (key == "emg_block_fcg_check_every") o.block_fcg_check_every = geti(k, v);
     else if (key == "emg_spmm_tiled") o.spmm_tiled = v.empty() ? 1 : getb(v);
     else if (key == "emg_tiled_smem_kb") o.tiled_smem_kb = geti(k, v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
@@ -233,6 +234,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else fail(EMG_ERR_OPTION, "unknown option %s", k.c_str());
   }
   if (o.gmres_restart < 1 || o.gmres_restart > 32) fail(EMG_ERR_OPTION, "A_ksp_gmres_restart must be in [1, 32]");
+  if (o.block_fcg_check_every < 1) fail(EMG_ERR_OPTION, "-emg_block_fcg_check_every must be >= 1");
   if (o.fcg_mmax < 1 || o.fcg_mmax > 30 || o.block_fcg_mmax < 1 || o.block_fcg_mmax > 30)
     fail(EMG_ERR_OPTION, "FCG truncation lengths must be in [1, 30]");
   if (o.ams_relax_times < 1 || o.amg_relax_times < 1) fail(EMG_ERR_OPTION, "relax times must be >= 1");
@@ -631,6 +633,7 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_block_inner_rtol") *value = o.block_inner_rtol;
   else if (k == "emg_block_inner_max_it") *value = o.block_inner_max_it;
   else if (k == "emg_block_fcg_mmax") *value = o.block_fcg_mmax;
+  else if (k == "emg_block_fcg_check_every") *value = o.block_fcg_check_every;
   else if (k == "emg_spmm_tiled") *value = o.spmm_tiled;
   else if (k == "emg_tiled_smem_kb") *value = o.tiled_smem_kb;
   else fail(EMG_ERR_OPTION, "unknown option %s", key);
@@ -883,6 +886,7 @@ int emg_pc_apply_b(emg_context *c, const double *b, double *x) {
   w.vec_a.upload(bi, c->stream);
   w.vec_b.alloc((size_t)n * 2);
   w.fcg64.mmax = c->opt.fcg_mmax;
+  w.fcg64.check_every = 1;
   w.fcg64.solve(w.pams64, w.vec_a.p, w.vec_b.p, c->opt.inner_rtol, c->opt.inner_max_it, c->stream);
   std::vector<double> xo((size_t)n * 2);
   w.vec_b.download(xo.data(), xo.size(), c->stream);
@@ -920,6 +924,7 @@ int emg_solve_linear_system(emg_context *c, int target, const double *s_re, cons
   w.gm.restart = c->opt.gmres_restart;
   w.gm.omega.upload(&c->omega, 1, c->stream);
   w.fcg64.mmax = c->opt.fcg_mmax;
+  w.fcg64.check_every = 1;
   w.fcg64.total_its = 0;
   SolveStats st;
   auto pc = [&](const double *v, double *z) {
@@ -1285,6 +1290,7 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
   w.gm.restart = o.restart > 0 ? o.restart : c.opt.gmres_restart;
   w.gm.omega.upload(om, c.stream);
   w.fcg64.mmax = w.fcg32.mmax = c.opt.block_fcg_mmax;
+  w.fcg64.check_every = w.fcg32.check_every = c.opt.block_fcg_check_every;
   w.fcg64.verbose = w.fcg32.verbose = c.opt.verbose > 1;
   w.fcg64.total_its = w.fcg32.total_its = 0;
   if (fp32) {
@@ -1357,6 +1363,7 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
   if (infos)
     for (int j = 0; j < k; ++j) fill_info(&infos[j], st, inner, j);
   c.kernel_ms["solve_block"] = st.seconds * 1e3;
+  c.block_initial_res = st.initial_res;
 }
 
 // Any number of columns: blocks of at most kMaxBlock columns solved one after
@@ -1376,6 +1383,7 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
   Workspace &w = *c.ws;
   const size_t n = (size_t)c.ne;
   double total_s = 0;
+  std::vector<double> r0(k, 1.0);
   for (int j0 = 0; j0 < k; j0 += kMaxBlock) {
     const int kc = std::min(kMaxBlock, k - j0);
     int kb = 1;
@@ -1400,9 +1408,11 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
     total_s += c.kernel_ms["solve_block"] * 1e-3;
     if (infos)
       for (int j = 0; j < kc; ++j) infos[j0 + j] = inf[j];
+    for (int j = 0; j < kc && j < (int)c.block_initial_res.size(); ++j) r0[j0 + j] = c.block_initial_res[j];
   }
   EMG_CUDA(cudaStreamSynchronize(c.stream));
   c.kernel_ms["solve_block"] = total_s * 1e3;
+  c.block_initial_res = r0;
 }
 
 int emg_solve_block_dev(emg_context *c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
@@ -1438,6 +1448,14 @@ int emg_spmv_complex_dev(emg_context *c, int k, const double *omegas, const doub
   c->ws->omega_k.upload(omegas, k, c->stream);
   spmm_complex(c->ne, k, c->rp.p, c->ci.p, c->Cv.p, c->Msv.p, c->ws->omega_k.p, x_dev, nullptr, y_dev, false,
                conj_out != 0, c->stream);
+  EMG_API_END
+}
+
+int emg_last_initial_residuals(emg_context *c, int k, double *rel) {
+  EMG_API_BEGIN
+  need(c && rel && k >= 0, EMG_ERR_ARG, "null argument");
+  need((size_t)k <= c->block_initial_res.size(), EMG_ERR_STATE, "no block solve of that width yet");
+  std::copy(c->block_initial_res.begin(), c->block_initial_res.begin() + k, rel);
   EMG_API_END
 }
 

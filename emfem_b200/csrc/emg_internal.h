@@ -181,6 +181,7 @@ struct Options {
   double block_inner_rtol = 1e-2;
   int block_inner_max_it = 30;
   int block_fcg_mmax = 2;
+  int block_fcg_check_every = 5;  // inner iterations between host looks at the column status
   int spmm_tiled = 0;         // edge-column SpMMs gather through per-tile shared memory
   int tiled_smem_kb = 64;     // shared memory budget of one tile
   int verbose = 0;
@@ -240,6 +241,8 @@ struct Context {
   std::map<int, DBuf<double>> sol;
   // timing
   std::map<std::string, double> kernel_ms;
+  // per column of the last block solve: ||b - A x0|| / ||b|| of its start
+  std::vector<double> block_initial_res;
   // rank of each boundary edge among the boundary edges (-1 elsewhere)
   std::vector<int> h_bnd_rank;
   DBuf<int> bnd_rank;
@@ -249,6 +252,8 @@ struct Context {
   // tiled copies of the fixed patterns, keyed by (row pointer, bytes per x row)
   std::map<std::pair<const int *, int>, std::unique_ptr<TiledPattern>> tiles;
   std::unique_ptr<Workspace> ws;
+  // learned warm start (network, optimiser state, per-edge features), built on first use
+  std::shared_ptr<struct WarmStartNet> warm;
   Context();
   ~Context();
 };

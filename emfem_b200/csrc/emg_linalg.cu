@@ -32,6 +32,28 @@ void spmm_launch(const SpmmArgs &a, cudaStream_t s) {
   spmm_kernel<T, K, V, NL><<<grid, 256, 0, s>>>(a);
 }
 
+// row-group kernel (spmm_rows_kernel): nl = -B selects it with B gathers in
+// flight per lane
+template <typename T, int K, int V, int B>
+constexpr bool spmm_rows_legal() {
+  return (K % V) == 0 && (K / V) <= 32 && (32 % (K / V)) == 0 && ((K / V) % B) == 0 && sizeof(T) * V <= 16;
+}
+
+template <typename T, int K, int V, int B>
+void spmm_rows_launch(const SpmmArgs &a, cudaStream_t s) {
+  constexpr int RPW = 32 / (K / V);
+  long warps = ((long)a.n + RPW - 1) / RPW;
+  unsigned grid = (unsigned)((warps * 32 + 255) / 256);
+  if (grid == 0) return;
+  spmm_rows_kernel<T, K, V, B><<<grid, 256, 0, s>>>(a);
+}
+
+template <typename T, int K, int V, int B>
+SpmmFn spmm_rows_pick() {
+  if constexpr (spmm_rows_legal<T, K, V, B>()) return &spmm_rows_launch<T, K, V, B>;
+  else return nullptr;
+}
+
 template <typename T, int K, int V, int NL>
 SpmmFn spmm_pick() {
   if constexpr (spmm_legal<T, K, V, NL>()) return &spmm_launch<T, K, V, NL>;
@@ -40,6 +62,8 @@ SpmmFn spmm_pick() {
 template <typename T, int K, int V>
 SpmmFn spmm_pick_nl(int nl) {
   switch (nl) {
+  case -4: return spmm_rows_pick<T, K, V, 4>();
+  case -8: return spmm_rows_pick<T, K, V, 8>();
   case 1: return spmm_pick<T, K, V, 1>();
   case 2: return spmm_pick<T, K, V, 2>();
   case 4: return spmm_pick<T, K, V, 4>();
@@ -123,7 +147,7 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
       EMG_CUDA(cudaEventCreate(&e1));
       float bestms = 1e30f;
       for (int v : {1, 2, 4})
-        for (int nl : {1, 2, 4, 8, 16, 32}) {
+        for (int nl : {1, 2, 4, 8, 16, 32, -4, -8}) {
           SpmmFn f = spmm_fn<T>(K, v, nl);
           if (!f) continue;
           f(a, s);  // warm-up

@@ -237,6 +237,68 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
   spmm_epilogue<T, K, V>(a, row, cb, acc, w, two);
 }
 
+// Row-group SpMM: G = K / V lanes serve one row (lane j owns column block j),
+// 32 / G rows per warp.  A row's nonzeros are loaded cooperatively, G at a
+// time (lane j loads nonzero j of the chunk: index and both value parts in
+// coalesced loads, no dependent rounds), then broadcast with warp shuffles,
+// so that B gathers of x rows per lane are in flight at once.  Trip counts are
+// uniform across the warp (the longest row of the warp sets them); entries
+// past a row's end have zero coefficients and issue no gather.
+template <typename T, int K, int V, int B>
+__global__ void __launch_bounds__(256) spmm_rows_kernel(SpmmArgs a) {
+  constexpr int G = K / V;
+  constexpr int RPW = 32 / G;
+  static_assert(G <= 32 && (32 % G) == 0 && (G % B) == 0, "bad row-group layout");
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int grp = lane / G, j = lane % G;
+  const int row = gw * RPW + grp;
+  const bool valid = row < a.n;
+  const T *__restrict__ vc = static_cast<const T *>(a.vc);
+  const T *__restrict__ vm = static_cast<const T *>(a.vm);
+  const T *__restrict__ x = static_cast<const T *>(a.x);
+  const bool two = vm != nullptr;
+  T w[V], acc[V];
+#pragma unroll
+  for (int i = 0; i < V; ++i) {
+    w[i] = two ? (T)__ldg(a.omega + j * V + i) : T(0);
+    acc[i] = T(0);
+  }
+  const int kb = valid ? __ldg(a.rp + row) : 0;
+  const int len = valid ? __ldg(a.rp + row + 1) - kb : 0;
+  int maxlen = len;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, off));
+  for (int c0 = 0; c0 < maxlen; c0 += G) {
+    const bool ok = c0 + j < len;
+    const int cj = ok ? __ldg(a.ci + kb + c0 + j) : 0;
+    const T cc = ok ? __ldg(vc + kb + c0 + j) : T(0);
+    const T cm = (ok && two) ? __ldg(vm + kb + c0 + j) : T(0);
+#pragma unroll
+    for (int t0 = 0; t0 < G; t0 += B) {
+      T xv[B][V], ct[B], mt[B];
+#pragma unroll
+      for (int t = 0; t < B; ++t) {
+        const int src = grp * G + t0 + t;
+        const int jj = __shfl_sync(0xffffffffu, cj, src);
+        ct[t] = __shfl_sync(0xffffffffu, cc, src);
+        mt[t] = __shfl_sync(0xffffffffu, cm, src);
+        if (c0 + t0 + t < len) ldv<T, V>(x + (long)jj * K + j * V, xv[t]);
+        else {
+#pragma unroll
+          for (int i = 0; i < V; ++i) xv[t][i] = T(0);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < B; ++t)
+#pragma unroll
+        for (int i = 0; i < V; ++i) acc[i] = fma(two ? ct[t] + w[i] * mt[t] : ct[t], xv[t][i], acc[i]);
+    }
+  }
+  if (!valid) return;
+  spmm_epilogue<T, K, V>(a, row, j, acc, w, two);
+}
+
 // Row tiles with their own column lists: tile t covers rows [t R, t R + R);
 // its distinct columns are ucol[urp[t] .. urp[t+1]) (ascending), and lci[k]
 // is nonzero k's position in that list.  One CTA stages the x rows of its

@@ -810,6 +810,41 @@ int Fcg<T>::solve(Ams<T> &ams, const T *b, T *x, double rtol, int maxit, cudaStr
       [&](const T *p_, T *s_) { ams.spmm_B(SPMM_AX, p_, nullptr, s_, s); }, b, x, rtol, maxit, s);
 }
 
+// device-side column bookkeeping of the batched FCG: no host round trip per
+// iteration
+__global__ void fcg_init_kernel(int K, const double *__restrict__ bn, int *__restrict__ act, int *__restrict__ its,
+                                int *__restrict__ status) {
+  const int c = threadIdx.x;
+  if (c < K) {
+    act[c] = bn[c] > 0.0;
+    its[c] = 0;
+  }
+  if (c == 0) status[0] = status[1] = 0;
+}
+
+// after an update: count the iteration of every active column, retire the
+// converged ones (||r_c||^2 <= rtol^2 ||b_c||^2), flag NaN/Inf; status[0] =
+// active columns left, status[1] = 1 + the first non-finite column (0: none)
+__global__ void fcg_status_kernel(int K, const double *__restrict__ rn, const double *__restrict__ bn, double rtol2,
+                                  int *__restrict__ act, int *__restrict__ its, int *__restrict__ status) {
+  const int c = threadIdx.x;
+  int a = 0;
+  if (c < K && act[c]) {
+    its[c]++;
+    const double v = rn[c];
+    if (!isfinite(v)) {
+      atomicCAS(status + 1, 0, c + 1);
+      act[c] = 0;
+    } else if (v <= rtol2 * bn[c]) {
+      act[c] = 0;
+    } else {
+      a = 1;
+    }
+  }
+  const int n = __syncthreads_count(a);
+  if (c == 0) status[0] = n;
+}
+
 template <typename T>
 int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> &pc,
                        const std::function<void(const T *, T *)> &opB, const T *b, T *x, double rtol, int maxit,
@@ -817,8 +852,10 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
   K = Kc;
   const size_t N = (size_t)n * K;
   if (mmax < 1) mmax = 1;
+  if (K > 1024) fail(EMG_ERR_ARG, "batched FCG supports at most 1024 columns");
   r.alloc(N);
   z.alloc(N);
+  bool new_ring = false;
   if ((int)P.size() != mmax || P.empty() || P[0].n != N) {
     P.clear();
     S.clear();
@@ -828,6 +865,7 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
       P[j].alloc(N);
       S[j].alloc(N);
     }
+    new_ring = true;
   }
   dots.alloc((size_t)(mmax + 3) * K);
   eta.alloc((size_t)mmax * K);
@@ -836,8 +874,20 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
   beta.alloc((size_t)mmax * K);
   rn.alloc(K);
   bn.alloc(K);
-  ptrs.alloc(mmax);
-  DBuf<int> act(K);
+  act.alloc(K);
+  itsd.alloc(K);
+  status.alloc(2);
+  if (!h_status.p) EMG_CUDA(cudaMallocHost((void **)&h_status.p, 2 * sizeof(int)));
+  // ring orderings: for (head, nprev) the previous directions oldest first
+  if (new_ring || ptab_mmax != mmax || ptrs.n != (size_t)mmax * (mmax + 1) * mmax) {
+    std::vector<T *> tab((size_t)mmax * (mmax + 1) * mmax, nullptr);
+    for (int h = 0; h < mmax; ++h)
+      for (int np = 1; np <= mmax; ++np)
+        for (int j = 0; j < np; ++j) tab[((size_t)h * (mmax + 1) + np) * mmax + j] = P[(h - np + j + mmax) % mmax].p;
+    ptrs.upload(tab, s);
+    EMG_CUDA(cudaStreamSynchronize(s));
+    ptab_mmax = mmax;
+  }
   its.assign(K, 0);
   fill_zero<T>((long)N, x, s);
   EMG_CUDA(cudaMemcpyAsync(r.p, b, sizeof(T) * N, cudaMemcpyDeviceToDevice, s));
@@ -847,38 +897,25 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
   }
   bn.zero(s);
   coldot<T>(n, K, b, b, bn.p, s);
-  std::vector<double> hbn(K), hrn(K);
-  bn.download(hbn.data(), K, s);
-  EMG_CUDA(cudaStreamSynchronize(s));
-  std::vector<int> active(K);
-  int nact = 0;
-  for (int c = 0; c < K; ++c) {
-    active[c] = hbn[c] > 0;
-    nact += active[c];
-  }
-  act.upload(active, s);
+  fcg_init_kernel<<<1, 1024, 0, s>>>(K, bn.p, act.p, itsd.p, status.p);
+  EMG_LAUNCH_CHECK();
+  const int every = std::max(1, check_every);
   int nprev = 0, head = 0, it = 0;
-  for (it = 0; it < maxit && nact > 0; ++it) {
+  for (it = 0; it < maxit; ++it) {
     pc(r.p, z.p);
-    // ring slots in age order; the new direction overwrites slot `head`
-    std::vector<T *> pj;
-    std::vector<int> slots;
-    for (int j = 0; j < nprev; ++j) {
-      int sl = (head - nprev + j + mmax) % mmax;
-      slots.push_back(sl);
-      pj.push_back(P[sl].p);
-    }
     if (nprev > 0) {
       EMG_CUDA(cudaMemsetAsync(dots.p, 0, sizeof(double) * nprev * K, s));
-      for (int j = 0; j < nprev; ++j) coldot<T>(n, K, z.p, S[slots[j]].p, dots.p + (size_t)j * K, s);
-      // eta of the ring slots in the same order
-      for (int j = 0; j < nprev; ++j)
-        EMG_CUDA(cudaMemcpyAsync(eord.p + (size_t)j * K, eta.p + (size_t)slots[j] * K, sizeof(double) * K,
+      for (int j = 0; j < nprev; ++j) {
+        const int sl = (head - nprev + j + mmax) % mmax;
+        coldot<T>(n, K, z.p, S[sl].p, dots.p + (size_t)j * K, s);
+        // eta of the ring slots in the same order
+        EMG_CUDA(cudaMemcpyAsync(eord.p + (size_t)j * K, eta.p + (size_t)sl * K, sizeof(double) * K,
                                  cudaMemcpyDeviceToDevice, s));
+      }
       fcg_beta_kernel<<<(nprev * K + 127) / 128, 128, 0, s>>>(K, nprev, dots.p, eord.p, act.p, beta.p);
       EMG_LAUNCH_CHECK();
-      ptrs.upload(pj.data(), nprev, s);
-      fcg_direction<T>(n, K, z.p, nprev, ptrs.p, beta.p, P[head].p, s);
+      fcg_direction<T>(n, K, z.p, nprev, ptrs.p + ((size_t)head * (mmax + 1) + nprev) * mmax, beta.p, P[head].p,
+                       s);
     } else {
       EMG_CUDA(cudaMemcpyAsync(P[head].p, z.p, sizeof(T) * N, cudaMemcpyDeviceToDevice, s));
     }
@@ -891,28 +928,36 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
     EMG_LAUNCH_CHECK();
     rn.zero(s);
     fcg_update<T>(n, K, alpha.p, p, sv, x, r.p, rn.p, s, r32);
+    fcg_status_kernel<<<1, 1024, 0, s>>>(K, rn.p, bn.p, rtol * rtol, act.p, itsd.p, status.p);
+    EMG_LAUNCH_CHECK();
     head = (head + 1) % mmax;
     nprev = std::min(nprev + 1, mmax);
-    rn.download(hrn.data(), K, s);
-    EMG_CUDA(cudaStreamSynchronize(s));
-    if (verbose) {
-      std::vector<double> ha(K);
-      alpha.download(ha.data(), K, s);
+    // the host looks at the column status only every `every` iterations (and
+    // at the cap); columns that converged in between stay frozen (alpha = beta
+    // = 0 keeps x and r)
+    if (verbose || (it + 1) % every == 0 || it + 1 == maxit) {
+      EMG_CUDA(cudaMemcpyAsync(h_status.p, status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
       EMG_CUDA(cudaStreamSynchronize(s));
-      fprintf(stderr, "fcg it %d:", it);
-      for (int c = 0; c < K; ++c) fprintf(stderr, " [%d a=%.3e r=%.3e]", c, ha[c], std::sqrt(hrn[c] / std::max(hbn[c], 1e-300)));
-      fprintf(stderr, "\n");
+      if (verbose) {
+        std::vector<double> ha(K), hrn(K), hbn(K);
+        alpha.download(ha.data(), K, s);
+        rn.download(hrn.data(), K, s);
+        bn.download(hbn.data(), K, s);
+        EMG_CUDA(cudaStreamSynchronize(s));
+        fprintf(stderr, "fcg it %d:", it);
+        for (int c = 0; c < K; ++c)
+          fprintf(stderr, " [%d a=%.3e r=%.3e]", c, ha[c], std::sqrt(hrn[c] / std::max(hbn[c], 1e-300)));
+        fprintf(stderr, "\n");
+      }
+      if (h_status.p[1]) fail(EMG_DIVERGED_NANORINF, "inner FCG: NaN or Inf in the residual of column %d",
+                              h_status.p[1] - 1);
+      if (h_status.p[0] == 0) {
+        ++it;
+        break;
+      }
     }
-    nact = 0;
-    for (int c = 0; c < K; ++c) {
-      if (!active[c]) continue;
-      its[c]++;
-      if (!std::isfinite(hrn[c])) fail(EMG_DIVERGED_NANORINF, "inner FCG: NaN or Inf in the residual of column %d", c);
-      if (hrn[c] <= rtol * rtol * hbn[c]) active[c] = 0;
-      nact += active[c];
-    }
-    act.upload(active, s);
   }
+  itsd.download(its.data(), K, s);
   EMG_CUDA(cudaStreamSynchronize(s));
   long tot = 0;
   for (int c = 0; c < K; ++c) tot += its[c];
@@ -924,6 +969,17 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
 // batched FGMRES (FP64)
 // ---------------------------------------------------------------------------
 typedef std::complex<double> zc;
+
+// x[:, c] *= keep[c] on an n x K complex block
+__global__ void column_mask_kernel(long n, int K, const double *__restrict__ keep, double2 *__restrict__ x) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n * K) return;
+  const double m = keep[i % K];
+  if (m != 1.0) {
+    double2 v = x[i];
+    x[i] = make_double2(v.x * m, v.y * m);
+  }
+}
 
 int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double rtol, int maxit, bool real_form,
                   const std::function<void(const double *, double *)> &precond, SolveStats &st) {
@@ -957,6 +1013,33 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
     if (bnorm[col] == 0) conv[col] = 1;
   }
   st.col_its.assign(k, 0);
+  st.initial_res.assign(k, 1.0);
+  if (use_guess) {
+    // the residual judges the guess: a column whose guess leaves a larger
+    // residual than zero starts from zero instead
+    spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, r.p, true, real_form, s);
+    nrm.zero(s);
+    cnorm2(n, k, r.p, nrm.p, s);
+    std::vector<double> r0(k);
+    nrm.download(r0.data(), k, s);
+    EMG_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> keep(k, 1.0);
+    bool drop = false;
+    for (int col = 0; col < k; ++col) {
+      const double rel = bnorm[col] > 0 ? std::sqrt(r0[col]) / bnorm[col] : 0.0;
+      st.initial_res[col] = rel;
+      if (!(rel <= 1.0)) {
+        keep[col] = 0.0;
+        st.initial_res[col] = 1.0;
+        drop = true;
+      }
+    }
+    if (drop) {
+      scale.upload(keep, s);
+      column_mask_kernel<<<(unsigned)(((long)n * k + 255) / 256), 256, 0, s>>>((long)n, k, scale.p, (double2 *)x);
+      EMG_LAUNCH_CHECK();
+    }
+  }
   int total = 0;
   std::vector<std::vector<zc>> H(k), cs(k), sn(k), g(k);
   auto all_conv = [&]() {

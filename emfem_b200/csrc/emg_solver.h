@@ -195,10 +195,14 @@ struct Fcg {
   DBuf<T> r, z, p;
   std::vector<DBuf<T>> P, S;  // previous directions and B-products (ring)
   DBuf<double> dots, eta, eord, alpha, beta, rn, bn;
-  DBuf<T *> ptrs;
+  DBuf<T *> ptrs;          // ring orderings of the previous directions, per (head, nprev)
+  int ptab_mmax = 0;
+  DBuf<int> act, itsd, status;  // per-column activity and iteration counts; active count, NaN flag
+  PinnedWord h_status;          // two words (see fcg_status_kernel)
   std::vector<int> its;
   long total_its = 0;
   int verbose = 0;
+  int check_every = 1;     // iterations between host looks at the column status
   int solve(Ams<T> &ams, const T *b, T *x, double rtol, int maxit, cudaStream_t s);
   // generic form: pc(r, z) applies the preconditioner, opB(p, s) the operator;
   // n rows, K columns
@@ -214,6 +218,7 @@ struct SolveStats {
   std::vector<double> true_res;  // per column
   std::vector<int> col_its;
   std::vector<int> converged;
+  std::vector<double> initial_res;  // per column: ||b - A x0|| / ||b|| of the start used
   double seconds = 0;
 };
 

@@ -314,11 +314,57 @@ int emg_assemble_rhs_dual_block_dev(emg_context *ctx, int k, int n_rx, const dou
 int emg_assemble_rhs_mt_block(emg_context *ctx, int k, const double *freqs, const int *modes, double *s);
 int emg_assemble_rhs_mt_block_dev(emg_context *ctx, int k, const double *freqs, const int *modes, double *s_dev);
 
+/* ---- learned warm start (no reference counterpart: the reference starts
+ * every FGMRES from zero, src/em_la.cc:49) ------------------------------
+ * A per-edge network (13 inputs: the two neighbour-frequency values of the
+ * edge scaled by their larger magnitude, log resistivities, log length,
+ * direction cosines, log distance to the source, log f and the position tau
+ * of f between the neighbours in log f; three hidden layers of 64 with GELU;
+ * BF16 weights, FP32 accumulation on the tensor cores) predicts a correction
+ * to the log-f interpolation of the two nearest solved frequencies of the
+ * same source.  Columns are (freqs[j], src[j]): src groups the columns of one
+ * source (MT polarisation or transmitter); src_pos (k x 3) gives point-source
+ * positions, NULL for plane waves (the distance feature is then the depth).
+ * The guess only moves iteration counts: emg_solve_block with use_guess
+ * falls back to zero for any column whose guess has a larger residual than
+ * zero, and every column is still solved to rtol. */
+typedef struct emg_warm_opts {
+  int steps;        /* Adam steps (minibatches)                              */
+  long batch;       /* samples (edge, column) per minibatch                  */
+  float lr;         /* Adam learning rate (decays over the last 30 %)        */
+  unsigned seed;    /* initialisation seed (first use of the network)        */
+} emg_warm_opts;
+
+/* trains on a solved block x_dev (n_edges x k complex): every column with a
+ * solved neighbour of the same source is a target; *final_loss: mean squared
+ * correction error of the last minibatch */
+int emg_warm_start_train(emg_context *ctx, int k, const double *freqs, const int *src, const double *src_pos,
+                         const double *x_dev, const emg_warm_opts *opts, double *final_loss);
+/* guesses for kt target columns into guess_dev (n_edges x kt complex);
+ * network 0: the log-f interpolation alone; a target without a solved
+ * column of its source gets zero */
+int emg_warm_start_predict(emg_context *ctx, int k, const double *freqs, const int *src, const double *src_pos,
+                           const double *x_dev, int kt, const double *tfreqs, const int *tsrc,
+                           const double *tsrc_pos, int network, double *guess_dev);
+/* the FP32 master parameters: W1 (64x16, out x in), W2, W3 (64x64), W4 (2x64),
+ * b1, b2, b3 (64), b4 (2); *nparam their count; get/set may be NULL */
+int emg_warm_start_params(emg_context *ctx, float *get, const float *set, int *nparam);
+/* gradients of one training minibatch (sample s: target s mod n_targets,
+ * a hashed edge of step `step`) without an update; tests */
+int emg_warm_start_gradients(emg_context *ctx, int k, const double *freqs, const int *src, const double *src_pos,
+                             const double *x_dev, long batch, int step, float *grads, double *loss);
+/* drops the network (the next use re-initialises it) */
+int emg_warm_start_reset(emg_context *ctx);
+
 /* ---- kernel-level entry points on device pointers (tests, benchmarks) -- */
 /* y = (C + i w Ms) x  (conj_out=0)  or its conjugate (conj_out=1, the
  * real-form operator of matshell_mult_a) for k complex columns. */
 int emg_spmv_complex_dev(emg_context *ctx, int k, const double *omegas_host, const double *x_dev,
                          double *y_dev, int conj_out);
+/* per column of the last emg_solve_block(_dev): the relative residual
+ * ||b - A x0|| / ||b|| of the start it used (1 for a zero start, also where
+ * a guess was worse than zero and was dropped) */
+int emg_last_initial_residuals(emg_context *ctx, int k, double *rel);
 /* per-kernel device timing of the last call of each kind (ms) */
 int emg_last_kernel_ms(emg_context *ctx, const char *name, double *ms);
 int emg_stream_synchronize(emg_context *ctx);

@@ -1,0 +1,165 @@
+"""Learned warm start: the tensor-core network against its CPU restatement
+(oracle/wsnet.py), and what it gains on a real solve.
+
+Tolerances: the device and the CPU round the same operands to BF16 and
+accumulate in FP32 in different orders, and a product rounded to BF16 can land
+on the other side of a rounding boundary; gradients and outputs therefore
+agree to 2e-3 of the largest value of each parameter group (an error in a
+layout or a transposition gives errors of order 1).  The interpolation-only
+guess has no BF16 step and agrees to 1e-6.
+"""
+
+import numpy as np
+import pytest
+
+import emfem_b200 as E
+from emfem_b200 import meshgen as mg
+import oracle.wsnet as W
+
+pytestmark = pytest.mark.gpu
+
+GROUPS = (("W1", 0, 1024), ("W2", 1024, 5120), ("W3", 5120, 9216), ("W4", 9216, 9344), ("b1", 9344, 9408),
+          ("b2", 9408, 9472), ("b3", 9472, 9536), ("b4", 9536, 9538))
+
+
+@pytest.fixture(scope="module")
+def small():
+    import torch
+    prob = mg.mt_halfspace_block(3000, freqs=(0.1, 1.0, 10.0), name="ws-small")
+    ne = prob.mesh.n_edges
+    rng = np.random.default_rng(7)
+    # smooth-ish complex columns: a few random modes of the edge midpoints
+    mid = 0.5 * (prob.mesh.points[prob.mesh.edges[:, 0]] + prob.mesh.points[prob.mesh.edges[:, 1]]) / 1e4
+    xs = np.zeros((ne, 6), dtype=np.complex128)
+    for j in range(6):
+        k = rng.normal(size=(3, 3))
+        xs[:, j] = (np.sin(mid @ k[0]) + 1j * np.cos(mid @ k[1])) * np.exp(0.1 * (mid @ k[2])) * 10.0 ** rng.uniform(-3, 3)
+    xs[rng.integers(0, ne, 20), :] = 0  # zero fields (homogeneous Dirichlet edges)
+    freqs = np.array([0.1, 1.0, 10.0, 0.1, 1.0, 10.0])
+    src = np.array([0, 0, 0, 1, 1, 1], dtype=np.int32)
+    c = E.EMContext(0)
+    c.set_mesh(prob.mesh)
+    c.set_model(prob.model)
+    c.set_frequencies(prob.survey.freqs)
+    c.create_linear_system(-3)
+    xd = torch.from_numpy(xs).to("cuda")
+    yield dict(prob=prob, ctx=c, xs=xs, xd=xd, freqs=freqs, src=src, rng=rng)
+    c.close()
+
+
+def _random_params(rng):
+    p = rng.normal(size=W.NPARAM).astype(np.float32) * 0.3
+    return p
+
+
+def test_gradients_match_cpu(small):
+    c, rng = small["ctx"], small["rng"]
+    params = _random_params(rng)
+    c.warm_start_params(set_to=params)
+    assert np.array_equal(c.warm_start_params(), params)
+    batch, step = 5000, 3  # a partial last tile
+    g, loss = c.warm_start_gradients(small["freqs"], small["src"], small["xd"].data_ptr(), batch, step)
+    specs = W.training_specs(list(small["freqs"]), list(small["src"]))
+    stat = W.edge_statics(small["prob"].mesh, small["prob"].model)
+    sp_idx, e_idx = W.batch_samples(len(specs), small["prob"].mesh.n_edges, batch, step)
+    X = np.zeros((batch, 16), dtype=np.float32)
+    T = np.zeros((batch, 2), dtype=np.float32)
+    for i, sp in enumerate(specs):
+        sel = np.nonzero(sp_idx == i)[0]
+        f, _, _, t = W.features(stat, small["xs"], sp, e_idx[sel], True)
+        X[sel], T[sel] = f, t
+    loss_c, g_c = W.gradients(params, X, T, np.float32(1.0 / batch))
+    assert abs(loss - loss_c) <= 1e-3 * abs(loss_c)
+    for name, a, b in GROUPS:
+        err = np.abs(g[a:b] - g_c[a:b]).max() / max(np.abs(g_c[a:b]).max(), 1e-30)
+        print("gradient %s: max %.3e rel err %.2e" % (name, np.abs(g_c[a:b]).max(), err))
+        assert err <= 2e-3, name
+
+
+def test_predictions_match_cpu(small):
+    import torch
+    c, rng = small["ctx"], small["rng"]
+    params = _random_params(rng)
+    c.warm_start_params(set_to=params)
+    ne = small["prob"].mesh.n_edges
+    # targets between the solved frequencies of each source
+    tf = np.array([0.3, 3.0, 0.05, 30.0])
+    ts = np.array([0, 1, 1, 0], dtype=np.int32)
+    stat = W.edge_statics(small["prob"].mesh, small["prob"].model)
+    for network in (False, True):
+        gd = torch.zeros((ne, tf.size), dtype=torch.complex128, device="cuda")
+        c.warm_start_predict(small["freqs"], small["src"], small["xd"].data_ptr(), tf, ts, gd.data_ptr(),
+                             network=network)
+        g = gd.cpu().numpy()
+        for j in range(tf.size):
+            cols = list(small["freqs"]) + [tf[j]]
+            srcs = list(small["src"]) + [ts[j]]
+            sp = [s for s in W.training_specs(cols, srcs) if s["tcol"] == len(cols) - 1][0]
+            f, base, sc, _ = W.features(stat, small["xs"], sp, np.arange(ne), False)
+            out = W.forward(params, f)[0] if network else np.zeros((ne, 2), np.float32)
+            ref = ((base[:, 0] + out[:, 0]).astype(np.float64) + 1j * (base[:, 1] + out[:, 1])) * sc
+            tol = 2e-3 if network else 1e-6
+            assert np.abs(g[:, j] - ref).max() <= tol * np.abs(ref).max(), (network, j)
+
+
+@pytest.fixture(scope="module")
+def ab_runs():
+    """Anchors (every other frequency, both polarisations) solved from zero;
+    the network trained on them; the other frequencies solved from zero,
+    from the log-f interpolation and from the network's guess."""
+    import torch
+    freqs = np.logspace(-2, 2, 7)
+    prob = mg.mt_halfspace_block(12000, with_block=False, n_bodies=4, topo_height=500.0, freqs=tuple(freqs),
+                                 seed=3, name="ws-ab")
+    ne = prob.mesh.n_edges
+    anchors = freqs[::2]
+    targets = freqs[1::2]
+    af, asrc = np.repeat(anchors, 2), np.tile(np.array([0, 1], np.int32), anchors.size)
+    tf, tsrc = np.repeat(targets, 2), np.tile(np.array([0, 1], np.int32), targets.size)
+    modes = lambda s: np.where(s == 0, E.XY_POLAR, E.YX_POLAR).astype(np.int32)
+    out = {}
+    with E.EMContext(0) as c:
+        c.set_mesh(prob.mesh)
+        c.set_model(prob.model)
+        c.set_frequencies(freqs)
+        c.create_linear_system(-3)
+        c.set_background(*mg.background_model(prob.mesh, prob.model))
+        c.assemble_matrix(0)
+        sa = torch.zeros((ne, af.size), dtype=torch.complex128, device="cuda")
+        xa = torch.zeros_like(sa)
+        c.assemble_rhs_mt_block_dev(af, modes(asrc), sa.data_ptr())
+        c.solve_block_dev(af, sa.data_ptr(), xa.data_ptr(), rtol=1e-8, max_it=200, inner_fp32=True)
+        out["loss"] = c.warm_start_train(af, asrc, xa.data_ptr(), steps=200, batch=32768, lr=2e-3, seed=5)
+        st = torch.zeros((ne, tf.size), dtype=torch.complex128, device="cuda")
+        c.assemble_rhs_mt_block_dev(tf, modes(tsrc), st.data_ptr())
+        for arm in ("zero", "interp", "network"):
+            x = torch.zeros_like(st)
+            if arm != "zero":
+                c.warm_start_predict(af, asrc, xa.data_ptr(), tf, tsrc, x.data_ptr(), network=(arm == "network"))
+            infos = c.solve_block_dev(tf, st.data_ptr(), x.data_ptr(), rtol=1e-8, max_it=200, inner_fp32=True,
+                                      use_guess=(arm != "zero"))
+            out[arm] = dict(its=[i.outer_its for i in infos], res=[i.true_rel_res for i in infos],
+                            ok=all(i.reason == 0 for i in infos), r0=c.last_initial_residuals(tf.size),
+                            x=x.cpu().numpy())
+    return out
+
+
+def test_warm_start_converges_to_the_same_fields(ab_runs):
+    z = ab_runs["zero"]["x"]
+    for arm in ("zero", "interp", "network"):
+        r = ab_runs[arm]
+        assert r["ok"] and max(r["res"]) <= 1e-8
+        for j in range(z.shape[1]):
+            assert np.abs(r["x"][:, j] - z[:, j]).max() <= 1e-6 * np.abs(z[:, j]).max()
+
+
+def test_warm_start_ab_iterations(ab_runs):
+    """A/B: outer iterations of the target columns from zero, from the log-f
+    interpolation and from the trained network's guess."""
+    for arm in ("zero", "interp", "network"):
+        r = ab_runs[arm]
+        print("%-8s outer its %s (total %d), initial residual %s" % (arm, r["its"], sum(r["its"]),
+                                                                   np.array2string(r["r0"], precision=2)))
+    print("training loss %.3e" % ab_runs["loss"])
+    assert np.all(ab_runs["network"]["r0"] <= 1.0)
+    assert sum(ab_runs["network"]["its"]) <= sum(ab_runs["zero"]["its"])
