@@ -981,11 +981,134 @@ __global__ void column_mask_kernel(long n, int K, const double *__restrict__ kee
   }
 }
 
+// Per-column Arnoldi bookkeeping of the block FGMRES on the device (one
+// thread per column): the Hessenberg columns, Givens rotations and the
+// rotated right-hand side g stay in device memory; the host reads two status
+// words per step (columns still iterating, NaN flag).
+struct GmDev {
+  double2 *H;      // K x (J+1) x J
+  double2 *cs, *sn;  // K x J
+  double2 *g;      // K x (J+1)
+  int *done, *jc, *colits, *conv;
+  const double *bnorm;
+  double *scale;   // K: divisor of the next basis vector (0: column finished)
+  int *status;     // [0] columns still iterating, [1] 1 + first column with NaN/Inf
+};
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double zabs(double2 a) { return hypot(a.x, a.y); }
+
+// start of a restart cycle: nrm2[c] = ||b - A x||^2
+__global__ void gm_start_kernel(int K, int J, const double *__restrict__ nrm2, double rtol, GmDev st) {
+  const int c = threadIdx.x;
+  int act = 0;
+  if (c < K) {
+    const double beta = sqrt(nrm2[c]);
+    if (!isfinite(beta)) atomicCAS(st.status + 1, 0, c + 1);
+    if (beta <= rtol * st.bnorm[c]) st.conv[c] = 1;
+    const bool cv = st.conv[c] != 0 || !isfinite(beta);
+    for (int i = 0; i <= J; ++i) st.g[(long)c * (J + 1) + i] = make_double2(0, 0);
+    st.g[(long)c * (J + 1)] = make_double2(cv ? 0.0 : beta, 0.0);
+    st.done[c] = cv;
+    st.jc[c] = 0;
+    st.scale[c] = cv ? 0.0 : beta;
+    act = !cv;
+  }
+  const int n = __syncthreads_count(act);
+  if (c == 0) st.status[0] = n;
+}
+
+__global__ void zero_imag_kernel(int n, double *__restrict__ h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) h[2 * i + 1] = 0.0;
+}
+
+// step j: h[i*K + c] (i <= j) = V_i^H w, hn[c] = ||w - sum h_i V_i||^2
+__global__ void gm_givens_kernel(int K, int J, int j, const double2 *__restrict__ h, const double *__restrict__ hn,
+                                 double rtol, GmDev st) {
+  const int c = threadIdx.x;
+  int act = 0;
+  if (c < K) {
+    const double hnext = sqrt(fmax(0.0, hn[c]));
+    if (!isfinite(hnext)) atomicCAS(st.status + 1, 0, c + 1);
+    st.scale[c] = isfinite(hnext) ? hnext : 0.0;
+    if (!st.done[c]) {
+      double2 *Hc = st.H + (long)c * (J + 1) * J;
+      double2 *cs = st.cs + (long)c * J, *sn = st.sn + (long)c * J, *g = st.g + (long)c * (J + 1);
+      for (int i = 0; i <= j; ++i) Hc[i * J + j] = h[i * K + c];
+      Hc[(j + 1) * J + j] = make_double2(hnext, 0.0);
+      for (int i = 0; i < j; ++i) {
+        const double2 a = Hc[i * J + j], b = Hc[(i + 1) * J + j];
+        const double2 t0 = zmul(cs[i], a), t1 = zmul(sn[i], b);
+        const double2 u0 = zmul(zconj(sn[i]), a), u1 = zmul(cs[i], b);
+        Hc[i * J + j] = make_double2(t0.x + t1.x, t0.y + t1.y);
+        Hc[(i + 1) * J + j] = make_double2(u1.x - u0.x, u1.y - u0.y);
+      }
+      const double2 a = Hc[j * J + j], b = Hc[(j + 1) * J + j];
+      const double aa = zabs(a);
+      const double rho = sqrt(a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y);
+      if (aa == 0.0) {
+        cs[j] = make_double2(0, 0);
+        sn[j] = make_double2(1, 0);
+      } else {
+        cs[j] = make_double2(aa / rho, 0);
+        const double2 ph = make_double2(a.x / aa, a.y / aa);
+        const double2 t = zmul(ph, zconj(b));
+        sn[j] = make_double2(t.x / rho, t.y / rho);
+      }
+      const double2 t0 = zmul(cs[j], a), t1 = zmul(sn[j], b);
+      Hc[j * J + j] = make_double2(t0.x + t1.x, t0.y + t1.y);
+      Hc[(j + 1) * J + j] = make_double2(0, 0);
+      const double2 gj = g[j];
+      const double2 gn = zmul(zconj(sn[j]), gj);
+      g[j + 1] = make_double2(-gn.x, -gn.y);
+      g[j] = zmul(cs[j], gj);
+      st.jc[c] = j + 1;
+      st.colits[c]++;
+      if (zabs(g[j + 1]) <= rtol * st.bnorm[c] || hnext == 0.0 || !isfinite(hnext)) st.done[c] = 1;
+      act = !st.done[c];
+    }
+  }
+  const int n = __syncthreads_count(act);
+  if (c == 0) st.status[0] = n;
+}
+
+// least-squares solutions of the cycle: y[i*K + c] (complex), zero past jc[c]
+__global__ void gm_lsq_kernel(int K, int J, int m, int real_form, GmDev st, double2 *__restrict__ y) {
+  const int c = threadIdx.x;
+  if (c >= K) return;
+  const double2 *Hc = st.H + (long)c * (J + 1) * J;
+  const double2 *g = st.g + (long)c * (J + 1);
+  const int mc = st.jc[c];
+  for (int i = m - 1; i >= 0; --i) {
+    if (i >= mc) {
+      y[i * K + c] = make_double2(0, 0);
+      continue;
+    }
+    double2 v = g[i];
+    for (int q = i + 1; q < mc; ++q) {
+      const double2 t = zmul(Hc[i * J + q], y[q * K + c]);
+      v.x -= t.x;
+      v.y -= t.y;
+    }
+    const double2 d = Hc[i * J + i];
+    const double dd = d.x * d.x + d.y * d.y;
+    double2 r = make_double2((v.x * d.x + v.y * d.y) / dd, (v.y * d.x - v.x * d.y) / dd);
+    if (real_form) r.y = 0.0;
+    y[i * K + c] = r;
+  }
+}
+
 int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double rtol, int maxit, bool real_form,
                   const std::function<void(const double *, double *)> &precond, SolveStats &st) {
   cudaStream_t s = c.stream;
   n = c.ne;
   const int J = restart;
+  if (J < 1 || J > 32) fail(EMG_ERR_ARG, "FGMRES restart must be in 1..32");
+  if (k > 1024) fail(EMG_ERR_ARG, "block FGMRES supports at most 1024 columns");
   const size_t N2 = (size_t)n * k * 2;  // doubles per block vector
   V.alloc(N2 * (J + 1));
   Z.alloc(N2 * J);
@@ -996,23 +1119,44 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   scale.alloc(k);
   y.alloc((size_t)J * k * 2);
   nrm.alloc(k);
+  bnd.alloc(k);
+  Hd.alloc((size_t)k * (J + 1) * J * 2);
+  csd.alloc((size_t)k * J * 2);
+  snd.alloc((size_t)k * J * 2);
+  gd.alloc((size_t)k * (J + 1) * 2);
+  ints.alloc((size_t)4 * k + 2);
+  if (!h_status.p) EMG_CUDA(cudaMallocHost((void **)&h_status.p, 2 * sizeof(int)));
+  GmDev gs;
+  gs.H = (double2 *)Hd.p;
+  gs.cs = (double2 *)csd.p;
+  gs.sn = (double2 *)snd.p;
+  gs.g = (double2 *)gd.p;
+  gs.done = ints.p;
+  gs.jc = ints.p + k;
+  gs.colits = ints.p + 2 * k;
+  gs.conv = ints.p + 3 * k;
+  gs.status = ints.p + 4 * k;
+  gs.bnorm = bnd.p;
+  gs.scale = scale.p;
+  ints.zero(s);
   if (!use_guess) fill_zero<double>((long)N2, x, s);
   cudaEvent_t e0, e1;
   EMG_CUDA(cudaEventCreate(&e0));
   EMG_CUDA(cudaEventCreate(&e1));
   EMG_CUDA(cudaEventRecord(e0, s));
-  std::vector<double> hb(k), hbeta(k), hhn(k), hh((size_t)(J + 1) * k * 2);
+  std::vector<double> hb(k);
   nrm.zero(s);
   cnorm2(n, k, b, nrm.p, s);
   nrm.download(hb.data(), k, s);
   EMG_CUDA(cudaStreamSynchronize(s));
   std::vector<double> bnorm(k);
-  std::vector<int> conv(k, 0);
+  std::vector<int> conv0(k, 0);
   for (int col = 0; col < k; ++col) {
     bnorm[col] = std::sqrt(hb[col]);
-    if (bnorm[col] == 0) conv[col] = 1;
+    if (bnorm[col] == 0) conv0[col] = 1;
   }
-  st.col_its.assign(k, 0);
+  bnd.upload(bnorm, s);
+  EMG_CUDA(cudaMemcpyAsync(gs.conv, conv0.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
   st.initial_res.assign(k, 1.0);
   if (use_guess) {
     // the residual judges the guess: a column whose guess leaves a larger
@@ -1041,37 +1185,20 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
     }
   }
   int total = 0;
-  std::vector<std::vector<zc>> H(k), cs(k), sn(k), g(k);
-  auto all_conv = [&]() {
-    for (int col = 0; col < k; ++col)
-      if (!conv[col]) return false;
-    return true;
+  auto read_status = [&]() {
+    EMG_CUDA(cudaMemcpyAsync(h_status.p, gs.status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    EMG_CUDA(cudaStreamSynchronize(s));
+    if (h_status.p[1]) fail(EMG_DIVERGED_NANORINF, "FGMRES: NaN or Inf in the residual of column %d", h_status.p[1] - 1);
+    return h_status.p[0];
   };
-  while (total < maxit && !all_conv()) {
+  while (total < maxit) {
     spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, r.p, true, real_form, s);
     nrm.zero(s);
     cnorm2(n, k, r.p, nrm.p, s);
-    nrm.download(hbeta.data(), k, s);
-    EMG_CUDA(cudaStreamSynchronize(s));
-    for (int col = 0; col < k; ++col) {
-      hbeta[col] = std::sqrt(hbeta[col]);
-      if (!std::isfinite(hbeta[col])) fail(EMG_DIVERGED_NANORINF, "FGMRES: NaN or Inf in the residual");
-      if (hbeta[col] <= rtol * bnorm[col]) conv[col] = 1;
-    }
-    if (all_conv()) break;
-    std::vector<double> sc(k);
-    for (int col = 0; col < k; ++col) sc[col] = conv[col] ? 0.0 : hbeta[col];
-    scale.upload(sc, s);
+    gm_start_kernel<<<1, 1024, 0, s>>>(k, J, nrm.p, rtol, gs);
+    EMG_LAUNCH_CHECK();
+    if (read_status() == 0) break;
     cscale(n, k, r.p, scale.p, V.p, s);
-    std::vector<int> jc(k, 0), done(k, 0);
-    for (int col = 0; col < k; ++col) {
-      H[col].assign((size_t)(J + 1) * J, zc(0));
-      cs[col].assign(J, zc(0));
-      sn[col].assign(J, zc(0));
-      g[col].assign(J + 1, zc(0));
-      g[col][0] = conv[col] ? 0.0 : hbeta[col];
-      done[col] = conv[col];
-    }
     int j;
     for (j = 0; j < J && total < maxit; ++j) {
       double *Vj = V.p + N2 * j;
@@ -1079,77 +1206,27 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
       precond(Vj, Zj);
       spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, Zj, nullptr, w.p, false, real_form, s);
       cmultidot(n, k, j + 1, V.p, (long)N2, w.p, h.p, nullptr, 0, s);
-      h.download(hh.data(), (size_t)(j + 1) * k * 2, s);
-      EMG_CUDA(cudaStreamSynchronize(s));
       if (real_form) {
-        for (size_t q = 0; q < (size_t)(j + 1) * k; ++q) hh[2 * q + 1] = 0.0;
-        h.upload(hh.data(), (size_t)(j + 1) * k * 2, s);
+        zero_imag_kernel<<<((j + 1) * k + 255) / 256, 256, 0, s>>>((j + 1) * k, h.p);
+        EMG_LAUNCH_CHECK();
       }
       cgs_update(n, k, j + 1, V.p, (long)N2, h.p, w.p, hn.p, s);
-      hn.download(hhn.data(), k, s);
-      EMG_CUDA(cudaStreamSynchronize(s));
-      std::vector<double> hnext(k);
-      for (int col = 0; col < k; ++col) hnext[col] = std::sqrt(std::max(0.0, hhn[col]));
-      scale.upload(hnext, s);
+      gm_givens_kernel<<<1, 1024, 0, s>>>(k, J, j, (const double2 *)h.p, hn.p, rtol, gs);
+      EMG_LAUNCH_CHECK();
       cscale(n, k, w.p, scale.p, V.p + N2 * (j + 1), s);
       ++total;
-      bool all_done = true;
-      for (int col = 0; col < k; ++col) {
-        if (done[col]) continue;
-        std::vector<zc> &Hc = H[col];
-        for (int i = 0; i <= j; ++i) Hc[(size_t)i * J + j] = zc(hh[2 * (i * k + col)], hh[2 * (i * k + col) + 1]);
-        Hc[(size_t)(j + 1) * J + j] = hnext[col];
-        for (int i = 0; i < j; ++i) {
-          zc a = Hc[(size_t)i * J + j], bb = Hc[(size_t)(i + 1) * J + j];
-          Hc[(size_t)i * J + j] = cs[col][i] * a + sn[col][i] * bb;
-          Hc[(size_t)(i + 1) * J + j] = -std::conj(sn[col][i]) * a + cs[col][i] * bb;
-        }
-        zc a = Hc[(size_t)j * J + j], bb = Hc[(size_t)(j + 1) * J + j];
-        double rho = std::sqrt(std::norm(a) + std::norm(bb));
-        if (std::abs(a) == 0.0) {
-          cs[col][j] = 0.0;
-          sn[col][j] = 1.0;
-        } else {
-          cs[col][j] = std::abs(a) / rho;
-          sn[col][j] = (a / std::abs(a)) * std::conj(bb) / rho;
-        }
-        Hc[(size_t)j * J + j] = cs[col][j] * a + sn[col][j] * bb;
-        Hc[(size_t)(j + 1) * J + j] = 0.0;
-        g[col][j + 1] = -std::conj(sn[col][j]) * g[col][j];
-        g[col][j] = cs[col][j] * g[col][j];
-        jc[col] = j + 1;
-        st.col_its[col]++;
-        if (std::abs(g[col][j + 1]) <= rtol * bnorm[col] || hnext[col] == 0.0) done[col] = 1;
-        if (!done[col]) all_done = false;
-      }
-      if (all_done) {
+      // one status read per step: a further step would cost a whole inner
+      // solve, far more than waiting for two words
+      if (read_status() == 0) {
         ++j;
         break;
       }
     }
-    // least-squares solutions, one per column
-    int jmax = 0;
-    std::vector<double> hy((size_t)J * k * 2, 0.0);
-    for (int col = 0; col < k; ++col) {
-      int m = jc[col];
-      jmax = std::max(jmax, m);
-      std::vector<zc> yy(m);
-      for (int i = m - 1; i >= 0; --i) {
-        zc v = g[col][i];
-        for (int q = i + 1; q < m; ++q) v -= H[col][(size_t)i * J + q] * yy[q];
-        yy[i] = v / H[col][(size_t)i * J + i];
-      }
-      for (int i = 0; i < m; ++i) {
-        hy[2 * ((size_t)i * k + col)] = yy[i].real();
-        hy[2 * ((size_t)i * k + col) + 1] = real_form ? 0.0 : yy[i].imag();
-      }
+    if (j > 0) {
+      gm_lsq_kernel<<<1, 1024, 0, s>>>(k, J, j, real_form ? 1 : 0, gs, (double2 *)y.p);
+      EMG_LAUNCH_CHECK();
+      cupdate(n, k, j, Z.p, (long)N2, y.p, x, s);
     }
-    if (jmax > 0) {
-      y.upload(hy.data(), (size_t)jmax * k * 2, s);
-      cupdate(n, k, jmax, Z.p, (long)N2, y.p, x, s);
-    }
-    EMG_CUDA(cudaStreamSynchronize(s));
-    (void)done;
   }
   // true residual in FP64
   spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, r.p, true, real_form, s);
@@ -1157,6 +1234,8 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   cnorm2(n, k, r.p, nrm.p, s);
   std::vector<double> tr(k);
   nrm.download(tr.data(), k, s);
+  st.col_its.assign(k, 0);
+  EMG_CUDA(cudaMemcpyAsync(st.col_its.data(), gs.colits, sizeof(int) * k, cudaMemcpyDeviceToHost, s));
   EMG_CUDA(cudaEventRecord(e1, s));
   EMG_CUDA(cudaEventSynchronize(e1));
   float ms = 0;

@@ -230,6 +230,9 @@ struct SolveStats {
 struct Fgmres {
   int n = 0, k = 0, restart = 30;
   DBuf<double> V, Z, w, r, h, hn, scale, y, omega, nrm;
+  DBuf<double> bnd, Hd, csd, snd, gd;  // per-column norms, Hessenberg, rotations, rotated rhs (device)
+  DBuf<int> ints;                      // done, jc, its, conv per column; two status words
+  PinnedWord h_status;
   int solve(Context &c, const double *b, double *x, bool use_guess, double rtol, int maxit, bool real_form,
             const std::function<void(const double *, double *)> &precond, SolveStats &st);
 };
