@@ -222,6 +222,8 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_fused_vcycle") o.ams_fused = v.empty() ? 1 : getb(v);
     else if (key == "emg_fused_blocks_per_sm") o.fused_bps = geti(k, v);
     else if (key == "emg_fused_rows") o.fused_rows = geti(k, v);
+    else if (key == "emg_fused_wait_ms") o.fused_wait_ms = getr(k, v);
+    else if (key == "emg_fused_test_withhold") o.fused_test_withhold = geti(k, v);
     else if (key == "emg_pi_coupled") o.pi_coupled = v.empty() ? 1 : getb(v);
     else if (key == "emg_block_inner_rtol") o.block_inner_rtol = getr(k, v);
     else if (key == "emg_block_inner_max_it") o.block_inner_max_it = geti(k, v);
@@ -629,6 +631,8 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_fused_vcycle") *value = o.ams_fused;
   else if (k == "emg_fused_blocks_per_sm") *value = o.fused_bps;
   else if (k == "emg_fused_rows") *value = o.fused_rows;
+  else if (k == "emg_fused_wait_ms") *value = o.fused_wait_ms;
+  else if (k == "emg_fused_test_withhold") *value = o.fused_test_withhold;
   else if (k == "emg_pi_coupled") *value = o.pi_coupled;
   else if (k == "emg_block_inner_rtol") *value = o.block_inner_rtol;
   else if (k == "emg_block_inner_max_it") *value = o.block_inner_max_it;

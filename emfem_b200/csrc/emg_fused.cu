@@ -71,7 +71,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // every waiter.  Returns false when the launch must stop.
 constexpr int EMG_FUSED_TIMEOUT = 1;
 
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+// withhold: the last block to arrive does not publish the next generation
+// (a test of the bounded wait: the others wait for a flag that nothing sets)
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned long long wait_ns, bool withhold) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -79,10 +81,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
     const unsigned g = ld_acquire(bar + 1);
     __threadfence();
     const unsigned arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
+    if (arrived == gridDim.x - 1 && !withhold) {
       atomicExch(bar, 0u);
       __threadfence();
       st_release(bar + 1, g + 1);
+    } else if (arrived == gridDim.x - 1) {
+      // the withheld release: this block goes on; its next barrier waits
     } else {
       const unsigned long long t0 = global_ns();
       for (unsigned it = 0;; ++it) {
@@ -91,7 +95,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
           ok = 0;
           break;
         }
-        if (it > (1u << 22) || global_ns() - t0 > 2000000000ull) {
+        if (it > (1u << 22) || global_ns() - t0 > wait_ns) {
           atomicCAS(err, 0, EMG_FUSED_TIMEOUT);
           ok = 0;
           break;
@@ -272,7 +276,8 @@ __device__ __forceinline__ void fused_coarse(const SpmmArgs &a) {
 
 template <typename T, int K>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) vcycle_fused_kernel(const FusedOp *__restrict__ ops, int nops,
-                                                              unsigned *bar, int *err) {
+                                                              unsigned *bar, int *err, unsigned long long wait_ns,
+                                                              int withhold_first) {
   __shared__ FusedOp sop;
   for (int i = 0; i < nops; ++i) {
     if (threadIdx.x == 0) sop = ops[i];
@@ -283,12 +288,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) vcycle_fused_kern
     case FOP_JAC0_2: fused_jac0<T, K>(sop.a, true); break;
     default: fused_coarse<T, K>(sop.a); break;
     }
-    if (i + 1 < nops && !grid_barrier(bar, err)) return;
+    if (i + 1 < nops && !grid_barrier(bar, err, wait_ns, withhold_first && i == 0)) return;
   }
 }
 
 template <typename T, int K>
-void fused_launch_k(const FusedOp *ops, int nops, unsigned *bar, int *err, int max_bps, cudaStream_t s) {
+void fused_launch_k(const FusedOp *ops, int nops, unsigned *bar, int *err, int max_bps, cudaStream_t s,
+                    unsigned long long wait_ns, int withhold) {
   // co-resident grid: the occupancy limit of the kernel on every SM
   static std::map<std::pair<int, int>, int> blocks_for;  // (device, max_bps) -> blocks
   int dev = 0;
@@ -317,28 +323,31 @@ void fused_launch_k(const FusedOp *ops, int nops, unsigned *bar, int *err, int m
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  EMG_CUDA(cudaLaunchKernelEx(&cfg, vcycle_fused_kernel<T, K>, ops, nops, bar, err));
+  EMG_CUDA(cudaLaunchKernelEx(&cfg, vcycle_fused_kernel<T, K>, ops, nops, bar, err, wait_ns, withhold));
   EMG_LAUNCH_CHECK();
 }
 
 }  // namespace
 
 template <typename T>
-void vcycle_fused(int K, const FusedOp *ops, int nops, unsigned *bar, int *err, int max_bps, cudaStream_t s) {
+void vcycle_fused(int K, const FusedOp *ops, int nops, unsigned *bar, int *err, int max_bps, cudaStream_t s,
+                  unsigned long long wait_ns, int withhold) {
   if (nops <= 0) return;
   switch (K) {
-  case 1: fused_launch_k<T, 1>(ops, nops, bar, err, max_bps, s); break;
-  case 2: fused_launch_k<T, 2>(ops, nops, bar, err, max_bps, s); break;
-  case 4: fused_launch_k<T, 4>(ops, nops, bar, err, max_bps, s); break;
-  case 8: fused_launch_k<T, 8>(ops, nops, bar, err, max_bps, s); break;
-  case 16: fused_launch_k<T, 16>(ops, nops, bar, err, max_bps, s); break;
-  case 32: fused_launch_k<T, 32>(ops, nops, bar, err, max_bps, s); break;
-  case 64: fused_launch_k<T, 64>(ops, nops, bar, err, max_bps, s); break;
+  case 1: fused_launch_k<T, 1>(ops, nops, bar, err, max_bps, s, wait_ns, withhold); break;
+  case 2: fused_launch_k<T, 2>(ops, nops, bar, err, max_bps, s, wait_ns, withhold); break;
+  case 4: fused_launch_k<T, 4>(ops, nops, bar, err, max_bps, s, wait_ns, withhold); break;
+  case 8: fused_launch_k<T, 8>(ops, nops, bar, err, max_bps, s, wait_ns, withhold); break;
+  case 16: fused_launch_k<T, 16>(ops, nops, bar, err, max_bps, s, wait_ns, withhold); break;
+  case 32: fused_launch_k<T, 32>(ops, nops, bar, err, max_bps, s, wait_ns, withhold); break;
+  case 64: fused_launch_k<T, 64>(ops, nops, bar, err, max_bps, s, wait_ns, withhold); break;
   default: fail(EMG_ERR_ARG, "unsupported block width K=%d", K);
   }
 }
 
-template void vcycle_fused<float>(int, const FusedOp *, int, unsigned *, int *, int, cudaStream_t);
-template void vcycle_fused<double>(int, const FusedOp *, int, unsigned *, int *, int, cudaStream_t);
+template void vcycle_fused<float>(int, const FusedOp *, int, unsigned *, int *, int, cudaStream_t, unsigned long long,
+                                  int);
+template void vcycle_fused<double>(int, const FusedOp *, int, unsigned *, int *, int, cudaStream_t, unsigned long long,
+                                   int);
 
 }  // namespace emg

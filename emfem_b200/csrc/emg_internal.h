@@ -175,6 +175,8 @@ struct Options {
   int ams_fused = 0;          // small nodal levels as one cooperative launch per V-cycle
   int fused_bps = 0;          // its resident blocks per SM cap (0: occupancy limit)
   int fused_rows = 1 << 30;   // levels below this many rows run fused
+  double fused_wait_ms = 2000;   // bound of a fused V-cycle's grid-barrier wait
+  int fused_test_withhold = 0;   // tests only: withhold the first barrier's release
   int pi_coupled = 0;         // vector Pi space with (1) or without (0) its x/y/z couplings
   // inner FCG of the batched path (emg_solve_block): a capped iteration count
   // per outer step; the flexible outer Krylov absorbs the inexactness

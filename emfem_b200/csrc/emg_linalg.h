@@ -91,8 +91,12 @@ void coarse_apply(int nc, int K, const double *inv, const int *col_slot, const T
 // zero before the first launch (every launch leaves them consistent); err:
 // set nonzero when a barrier wait gave up, which ends the launch early.
 // max_bps caps the resident blocks per SM (0: the occupancy limit).
+// wait_ns bounds every barrier wait; withhold != 0 (tests only) makes the
+// last block to arrive at the first barrier skip the release, so that the
+// others' waits run out
 template <typename T>
-void vcycle_fused(int K, const FusedOp *ops, int nops, unsigned *bar, int *err, int max_bps, cudaStream_t s);
+void vcycle_fused(int K, const FusedOp *ops, int nops, unsigned *bar, int *err, int max_bps, cudaStream_t s,
+                  unsigned long long wait_ns = 2000000000ull, int withhold = 0);
 
 // ---- complex (FP64) kernels of the outer FGMRES ------------------------------
 // y = b - A(w_c) x  or  y = A(w_c) x, complex n x K; conj_out conjugates the

@@ -112,9 +112,18 @@ __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::be
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// bounded wait for the mbarrier phase; false when it gave up
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait for the mbarrier phase (1 s of %globaltimer or 2^22 polls);
+// false when it gave up
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (int i = 0; i < (1 << 24); ++i) {
+  const unsigned long long t0 = global_ns();
+  for (int i = 0; i < (1 << 22); ++i) {
+    if ((i & 255) == 255 && global_ns() - t0 > 1000000000ull) return false;
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -310,7 +319,7 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(KArgs a) {
     }
     const bool done = mbar_wait(mbar, phase);
     ok = __syncthreads_and(ok && done) != 0;
-    phase ^= 1u;
+    if (ok) phase ^= 1u;  // after a failed wait the pending phase stays the one to wait for
     fence_after();
   };
   auto gemm = [&](uint32_t d, uint32_t a_off, int a_K, uint32_t b_off, int b_K, int K, int N, uint32_t acc0) {
@@ -456,6 +465,9 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(KArgs a) {
     if ((tid & 31) == 0) atomicAdd(a.loss, (double)l);
   }
   if (!ok && tid == 0) atomicExch(a.err, 1);
+  // a wait that gave up: wait once more (bounded) for the tensor-core work
+  // in flight before the tensor memory is released
+  if (NET && !ok) (void)mbar_wait(mbar, phase);
   if (NET) {
     fence_before();
     __syncthreads();

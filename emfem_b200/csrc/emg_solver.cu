@@ -166,6 +166,8 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   ams.fused = c.opt.ams_fused != 0;
   ams.fused_bps = c.opt.fused_bps;
   ams.fused_rows = c.opt.fused_rows;
+  ams.fused_wait_ns = (unsigned long long)(c.opt.fused_wait_ms * 1e6);
+  ams.fused_withhold = c.opt.fused_test_withhold;
   ams.fused_epoch = -1;
   // FP32 applications close with the gradient correction and hand it back
   // as a potential: after it, no FP32 product touches the (air) gradient
@@ -667,7 +669,7 @@ void Ams<T>::launch_fused(int sp, cudaStream_t s) {
   cudaEvent_t ev = nullptr;
   const char *bin = sizeof(T) == 4 ? "vcycle_fused_fp32" : "vcycle_fused_fp64";
   if (pf.enabled) pf.begin(bin, s, fops_bytes[sp], &ev);
-  vcycle_fused<T>(K, fops[sp].p, fops_n[sp], fbar.p, ferr.p, fused_bps, s);
+  vcycle_fused<T>(K, fops[sp].p, fops_n[sp], fbar.p, ferr.p, fused_bps, s, fused_wait_ns, fused_withhold);
   if (pf.enabled) pf.end(bin, s, ev);
 }
 

@@ -127,6 +127,8 @@ struct Ams {
   bool fused = false;
   int fused_bps = 0;               // resident blocks per SM cap (0: occupancy limit)
   int fused_rows = 1 << 30;        // levels with fewer rows run fused
+  unsigned long long fused_wait_ns = 2000000000ull;  // bound of every grid-barrier wait
+  int fused_withhold = 0;          // tests: the first barrier is never released
   int fused_from[NSUB] = {0, 0, 0, 0, 0};
   GraphCache graphs;
   std::vector<FusedOp> *rec = nullptr;  // set while vcycle() records instead of launching

@@ -126,3 +126,33 @@ def test_pi_vector_space_cycles(mt_small, extra):
         er, ei = c.get_solution(E.XY_POLAR)
         z = _direct(rp, ci, Cv, Mv, sr, si)
         assert np.abs((er + 1j * ei) - z).max() <= 1e-6 * np.abs(z).max()
+
+
+def test_fused_barrier_wait_runs_out_and_reports(mt_small):
+    """The fused V-cycle's grid-barrier waits are bounded: with the test-only
+    option that withholds the first barrier's release (the waiting blocks
+    wait for a flag that nothing sets) and a 1 ms bound, every waiter gives
+    up, the kernel ends, the error word is set and the solve returns
+    EMG_ERR_CUDA; a fresh context then solves normally."""
+    prob = mt_small
+    bg = mg.background_model(prob.mesh, prob.model)
+    freqs = [prob.survey.freqs[0], prob.survey.freqs[0]]
+    modes = [E.XY_POLAR, E.YX_POLAR]
+    for withhold in (1, 0):
+        with E.EMContext(0) as c:
+            c.process_options("-emg_fused_vcycle 1 -emg_fused_wait_ms 1 -emg_fused_test_withhold %d" % withhold)
+            c.set_mesh(prob.mesh)
+            c.set_model(prob.model)
+            c.set_frequencies(prob.survey.freqs)
+            c.create_linear_system(-3)
+            c.set_background(*bg)
+            c.assemble_matrix(0)
+            rhs = c.assemble_rhs_mt_block(freqs, modes)
+            if withhold:
+                with pytest.raises(E.EMGError) as ei:
+                    c.solve_block(freqs, rhs, rtol=1e-8, max_it=100, inner_fp32=True)
+                assert ei.value.code == E.api.EMG_ERR_CUDA
+                assert "timed out" in str(ei.value)
+            else:
+                x, infos = c.solve_block(freqs, rhs, rtol=1e-8, max_it=100, inner_fp32=True)
+                assert all(i.reason == 0 and i.true_rel_res <= 1e-8 for i in infos)
