@@ -111,6 +111,7 @@ _SIGS = {
     "emg_save_vtk": ([_P, C.c_char_p, _I, _P, _P], _I),
     "emg_interpolate_fields_block_dev": ([_P, _I, _P, _P, _I, _P, _P, _P], _I),
     "emg_last_initial_residuals": ([_P, _I, _P], _I),
+    "emg_amg_levels": ([_P, _I, _I, _D, _I, C.POINTER(_I), _P], _I),
     "emg_warm_start_train": ([_P, _I, _P, _P, _P, _P, C.POINTER(WarmOpts), C.POINTER(_D)], _I),
     "emg_warm_start_predict": ([_P, _I, _P, _P, _P, _P, _I, _P, _P, _P, _I, _P], _I),
     "emg_warm_start_params": ([_P, _P, _P, C.POINTER(_I)], _I),
@@ -532,6 +533,13 @@ class EMContext:
         """The dual right-hand side in all k columns of a device block."""
         r = _f64(np.asarray(rx).reshape(-1, 3))
         _check(lib().emg_assemble_rhs_dual_block_dev(self._h, int(k), r.shape[0], _ptr(r), C.c_void_p(s_ptr)))
+
+    def amg_levels(self, sp, gpu, w_ref):
+        """(rows, nnz A, nnz P, sum |A|, sum |P|) per level of a nodal hierarchy"""
+        out = np.zeros(5 * 64)
+        nl = C.c_int()
+        _check(lib().emg_amg_levels(self._h, int(sp), int(bool(gpu)), float(w_ref), 64, C.byref(nl), _ptr(out)))
+        return out[:5 * nl.value].reshape(nl.value, 5)
 
     def last_initial_residuals(self, k):
         out = np.zeros(int(k))

@@ -203,9 +203,12 @@ static void direct_interp(const HCsr &A, double w, const std::vector<int> &fn, c
     if ((int)row.size() > pmax) {
       double tot = 0, kept = 0;
       for (auto &p : row) tot += p.second;
+      // largest |w| first; equal magnitudes: the lower coarse column (the
+      // earlier entry of the row) first, so that the choice is deterministic
       std::partial_sort(row.begin(), row.begin() + pmax, row.end(),
                         [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
-                          return std::fabs(a.second) > std::fabs(b.second);
+                          const double fa = std::fabs(a.second), fb = std::fabs(b.second);
+                          return fa > fb || (fa == fb && a.first < b.first);
                         });
       row.resize(pmax);
       for (auto &p : row) kept += p.second;

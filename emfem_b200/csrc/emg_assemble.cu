@@ -442,14 +442,20 @@ __global__ void __launch_bounds__(128) assemble_nodal_kernel(ElemIn in, int nt, 
   }
 }
 
-void assemble_nodal(Context &c, HCsr out[4]) {
+void assemble_nodal_device(Context &c, DBuf<double> &buf) {
   long vnnz = c.h_vrp[c.nv];
-  DBuf<double> buf((size_t)vnnz * 8);
+  buf.alloc((size_t)vnnz * 8);
   buf.zero(c.stream);
   NodalOut o;
   for (int k = 0; k < 8; ++k) o.v[k] = buf.p + (size_t)k * vnnz;
   assemble_nodal_kernel<<<(unsigned)((c.nt + 127) / 128), 128, 0, c.stream>>>(elem_in(c), c.nt, c.vslot.p, o);
   EMG_LAUNCH_CHECK();
+}
+
+void assemble_nodal(Context &c, HCsr out[4]) {
+  long vnnz = c.h_vrp[c.nv];
+  DBuf<double> buf;
+  assemble_nodal_device(c, buf);
   // each part straight into its operator (no staging copy of all eight)
   for (int sp = 0; sp < 4; ++sp) {
     out[sp].n = out[sp].m = c.nv;

@@ -222,6 +222,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_fused_vcycle") o.ams_fused = v.empty() ? 1 : getb(v);
     else if (key == "emg_fused_blocks_per_sm") o.fused_bps = geti(k, v);
     else if (key == "emg_fused_rows") o.fused_rows = geti(k, v);
+    else if (key == "emg_gpu_amg") o.gpu_amg = v.empty() ? 1 : getb(v);
     else if (key == "emg_fused_wait_ms") o.fused_wait_ms = getr(k, v);
     else if (key == "emg_fused_test_withhold") o.fused_test_withhold = geti(k, v);
     else if (key == "emg_pi_coupled") o.pi_coupled = v.empty() ? 1 : getb(v);
@@ -631,6 +632,7 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_fused_vcycle") *value = o.ams_fused;
   else if (k == "emg_fused_blocks_per_sm") *value = o.fused_bps;
   else if (k == "emg_fused_rows") *value = o.fused_rows;
+  else if (k == "emg_gpu_amg") *value = o.gpu_amg;
   else if (k == "emg_fused_wait_ms") *value = o.fused_wait_ms;
   else if (k == "emg_fused_test_withhold") *value = o.fused_test_withhold;
   else if (k == "emg_pi_coupled") *value = o.pi_coupled;
@@ -1460,6 +1462,21 @@ int emg_last_initial_residuals(emg_context *c, int k, double *rel) {
   need(c && rel && k >= 0, EMG_ERR_ARG, "null argument");
   need((size_t)k <= c->block_initial_res.size(), EMG_ERR_STATE, "no block solve of that width yet");
   std::copy(c->block_initial_res.begin(), c->block_initial_res.begin() + k, rel);
+  EMG_API_END
+}
+
+int emg_amg_levels(emg_context *c, int sp, int gpu, double w_ref, int max_rows, int *nlev, double *out) {
+  EMG_API_BEGIN
+  need(c && nlev && out, EMG_ERR_ARG, "null argument");
+  need(c->assembled, EMG_ERR_STATE, "AMG levels before assemble_matrix");
+  need(sp >= 0 && sp < NSUB, EMG_ERR_ARG, "subspace index out of range");
+  use_device(*c);
+  std::vector<double> v;
+  amg_levels_report(*c, sp, gpu != 0, w_ref, v);
+  const int nl = (int)(v.size() / 5);
+  need(nl <= max_rows, EMG_ERR_ARG, "output holds too few levels");
+  *nlev = nl;
+  std::copy(v.begin(), v.end(), out);
   EMG_API_END
 }
 

@@ -169,6 +169,7 @@ struct Options {
   int amg_max_levels = 25;
   int amg_relax_times = 1;
   int smoother_cheb = 1;  // degree-2 Chebyshev (1) or l1-Jacobi (0) in AMS and AMG
+  int gpu_amg = 1;        // nodal AMG setup on the device (1) or on the host (0)
   // emg_*
   int inner_fp32 = 0;
   int graphs = 1;
@@ -281,6 +282,9 @@ void canonicalize(Context &c);            // device: sorted tets + canonical edg
 void build_slot_maps(Context &c);         // device: tet -> CSR slots
 void assemble_edge(Context &c);           // device: C, Ms, bdr cells
 void assemble_nodal(Context &c, HCsr out[4]);  // device + download (G, Pi_x, Pi_y, Pi_z)
+// the same on the device only: buf holds 8 vertex-pattern arrays, part p of
+// operator sp (G, Pi_x, Pi_y, Pi_z) at (2 sp + p) x nnz(vertex pattern)
+void assemble_nodal_device(Context &c, DBuf<double> &buf);
 // Pi^T K Pi, 3 nv rows, row 3 v + d; coupled = false keeps only the x/y/z
 // diagonal blocks (the three component spaces side by side, corrected at once)
 void assemble_pi_vector(Context &c, HCsr &out, bool coupled);

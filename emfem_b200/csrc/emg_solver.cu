@@ -19,6 +19,7 @@
 #include <numeric>
 #include <cstdio>
 
+#include "emg_amg_gpu.h"
 #include "emg_solver.h"
 
 namespace emg {
@@ -105,6 +106,37 @@ static void upload_csr(const HCsr &h, DCsr<T> &d, bool with_l1, cudaStream_t s) 
     else d.l1m.release();
   }
   EMG_CUDA(cudaStreamSynchronize(s));  // host temporaries go out of scope
+}
+
+// a device AMG level operator into the solver's precision, with l1 row sums
+template <typename T>
+static void to_level(GCsr &g, DCsr<T> &d, bool with_l1, cudaStream_t s) {
+  d.n = g.n;
+  d.m = g.m;
+  d.nnz = g.nnz;
+  const unsigned gn = (unsigned)((g.nnz + 255) / 256), gr = (unsigned)((g.n + 255) / 256);
+  d.vc.alloc(std::max<long>(g.nnz, 1));
+  combine_kernel<T><<<gn, 256, 0, s>>>(g.nnz, g.vc.p, nullptr, 0.0, d.vc.p);
+  if (g.vm.p) {
+    d.vm.alloc(std::max<long>(g.nnz, 1));
+    combine_kernel<T><<<gn, 256, 0, s>>>(g.nnz, g.vm.p, nullptr, 0.0, d.vm.p);
+  } else {
+    d.vm.release();
+  }
+  if (with_l1) {
+    d.l1c.alloc(g.n);
+    l1_rowsum_kernel<T><<<gr, 256, 0, s>>>(g.n, g.rp.p, g.vc.p, nullptr, 0.0, d.l1c.p);
+    if (g.vm.p) {
+      d.l1m.alloc(g.n);
+      l1_rowsum_kernel<T><<<gr, 256, 0, s>>>(g.n, g.rp.p, g.vm.p, nullptr, 0.0, d.l1m.p);
+    } else {
+      d.l1m.release();
+    }
+  }
+  EMG_LAUNCH_CHECK();
+  EMG_CUDA(cudaStreamSynchronize(s));  // g's values go out of scope with the level
+  d.rp = std::move(g.rp);
+  d.ci = std::move(g.ci);
 }
 
 // ---------------------------------------------------------------------------
@@ -245,6 +277,62 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   clk.lap("setup_gtb");
   HCsr nod[NSUB];
   const bool pi_coupled = c.opt.pi_coupled != 0;
+  AmgParams prm;
+  prm.theta = c.opt.amg_theta;
+  prm.pmax = c.opt.amg_pmax;
+  prm.max_coarse = c.opt.amg_max_coarse;
+  prm.max_levels = c.opt.amg_max_levels;
+  if (c.opt.gpu_amg && !pi_coupled) {
+    // nodal operators and their hierarchies built on the device
+    DBuf<double> parts;
+    assemble_nodal_device(c, parts);
+    EMG_CUDA(cudaStreamSynchronize(s));
+    clk.lap("setup_nodal");
+    double amg_ms = 0, conv_ms = 0;
+    for (int sp = 0; sp < NSUB; ++sp) {
+      auto &S = ams.sub[sp];
+      S.lv.clear();
+      S.coarse = HCsr();
+      S.nc = 0;
+      S.cinv.release();
+      S.cinv_w.clear();
+      if (!want[sp]) continue;
+      auto ta = std::chrono::steady_clock::now();
+      GCsr A0;
+      nodal_operator_gpu(c, parts, sp, A0, per_frequency ? w : -1.0);
+      AmgParams p2 = prm;
+      p2.seed = prm.seed + 7919ull * (uint64_t)sp;
+      p2.num_functions = sp == SUB_PIVEC ? 3 : 1;
+      std::vector<GpuLevel> glv;
+      GCsr gco;
+      amg_build_gpu(std::move(A0), w_ref, p2, glv, gco, s);
+      auto tb = std::chrono::steady_clock::now();
+      amg_ms += std::chrono::duration<double, std::milli>(tb - ta).count();
+      S.lv.resize(glv.size());
+      for (size_t l = 0; l < glv.size(); ++l) {
+        S.lv[l].nnzA = glv[l].A.nnz;
+        S.lv[l].nnzP = glv[l].P.nnz;
+        S.lv[l].nnzR = glv[l].R.nnz;
+        to_level<T>(glv[l].A, S.lv[l].A, true, s);
+        to_level<T>(glv[l].P, S.lv[l].P, false, s);
+        to_level<T>(glv[l].R, S.lv[l].R, false, s);
+      }
+      gcsr_to_host(gco, S.coarse, s);
+      S.nc = S.coarse.n;
+      conv_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+    }
+    c.kernel_ms["setup_amg"] = amg_ms;
+    c.kernel_ms["setup_upload"] = conv_ms;
+    for (int sp = 0; sp < NSUB; ++sp) {
+      ams.wb[sp].clear();
+      ams.wx[sp].clear();
+      ams.wr[sp].clear();
+      ams.wx2[sp].clear();
+      ams.wd[sp].clear();
+    }
+    ams.ws_K = 0;
+    return;
+  }
   if (want[0] || want[1] || want[2] || want[3] || (want[SUB_PIVEC] && !pi_coupled)) assemble_nodal(c, nod);
   if (want[SUB_PIVEC]) {
     if (pi_coupled) assemble_pi_vector(c, nod[SUB_PIVEC], true);
@@ -252,11 +340,6 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   }
   clk.lap("setup_nodal");
   double amg_ms = 0, upload_ms = 0;
-  AmgParams prm;
-  prm.theta = c.opt.amg_theta;
-  prm.pmax = c.opt.amg_pmax;
-  prm.max_coarse = c.opt.amg_max_coarse;
-  prm.max_levels = c.opt.amg_max_levels;
   for (int sp = 0; sp < NSUB; ++sp) {
     auto &S = ams.sub[sp];
     S.lv.clear();
@@ -1253,6 +1336,61 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   }
   st.outer_its = total;
   return total;
+}
+
+// per level of subspace sp's nodal hierarchy (built on the device or on the
+// host from the context's assembled operators): rows, nonzeros of A and P,
+// sums of |A| (both parts) and |P|; the coarsest operator adds a last row
+void amg_levels_report(Context &c, int sp, bool gpu, double w_ref, std::vector<double> &out) {
+  cudaStream_t s = c.stream;
+  AmgParams prm;
+  prm.theta = c.opt.amg_theta;
+  prm.pmax = c.opt.amg_pmax;
+  prm.max_coarse = c.opt.amg_max_coarse;
+  prm.max_levels = c.opt.amg_max_levels;
+  prm.seed = prm.seed + 7919ull * (uint64_t)sp;
+  prm.num_functions = sp == SUB_PIVEC ? 3 : 1;
+  std::vector<HCsr> As, Ps;
+  if (gpu) {
+    DBuf<double> parts;
+    assemble_nodal_device(c, parts);
+    GCsr A0;
+    nodal_operator_gpu(c, parts, sp, A0, -1.0);
+    std::vector<GpuLevel> glv;
+    GCsr gco;
+    amg_build_gpu(std::move(A0), w_ref, prm, glv, gco, s);
+    for (auto &L : glv) {
+      As.emplace_back();
+      Ps.emplace_back();
+      gcsr_to_host(L.A, As.back(), s);
+      gcsr_to_host(L.P, Ps.back(), s);
+    }
+    As.emplace_back();
+    gcsr_to_host(gco, As.back(), s);
+  } else {
+    HCsr nod[NSUB];
+    assemble_nodal(c, nod);
+    if (sp == SUB_PIVEC) interleave_components(nod + 1, nod[SUB_PIVEC]);
+    HostAmg h;
+    amg_build(std::move(nod[sp]), w_ref, prm, h);
+    for (auto &L : h.lv) {
+      As.push_back(std::move(L.A));
+      Ps.push_back(std::move(L.P));
+    }
+    As.push_back(std::move(h.coarse));
+  }
+  out.clear();
+  for (size_t l = 0; l < As.size(); ++l) {
+    const HCsr &A = As[l];
+    double sa = 0, sp_ = 0;
+    for (long k = 0; k < A.nnz(); ++k) sa += std::fabs(A.vc[k]) + (A.vm.empty() ? 0.0 : std::fabs(A.vm[k]));
+    long np = 0;
+    if (l < Ps.size()) {
+      np = Ps[l].nnz();
+      for (long k = 0; k < np; ++k) sp_ += std::fabs(Ps[l].vc[k]);
+    }
+    out.insert(out.end(), {(double)A.n, (double)A.nnz(), (double)np, sa, sp_});
+  }
 }
 
 template void ams_setup<float>(Context &, Ams<float> &, bool, double, double);

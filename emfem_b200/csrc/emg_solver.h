@@ -187,6 +187,10 @@ struct Ams {
 template <typename T>
 void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_ref);
 
+// tests: rows, nonzeros and absolute sums per level of a nodal hierarchy
+// built on the device (gpu) or on the host
+void amg_levels_report(Context &c, int sp, bool gpu, double w_ref, std::vector<double> &out);
+
 // batched FCG on B(w_c) with AMS, K real columns; returns per-column iteration
 // counts; x starts at zero.  Columns converge independently to
 // ||r_c|| <= rtol ||b_c|| (unpreconditioned norm, src/em_la.cc:120).

@@ -361,6 +361,12 @@ int emg_warm_start_reset(emg_context *ctx);
  * real-form operator of matshell_mult_a) for k complex columns. */
 int emg_spmv_complex_dev(emg_context *ctx, int k, const double *omegas_host, const double *x_dev,
                          double *y_dev, int conj_out);
+/* the nodal AMG hierarchy of AMS subspace sp (0 gradient, 1-3 Pi_x/y/z, 4 the
+ * vector space) of the assembled operators, built on the device (gpu != 0)
+ * or by the host build, for reference frequency w_ref: per level 5 values
+ * (rows, nonzeros of A, of P, sum |A| over both parts, sum |P|), the
+ * coarsest operator last; *nlev levels (at most max_rows).  Tests. */
+int emg_amg_levels(emg_context *ctx, int sp, int gpu, double w_ref, int max_rows, int *nlev, double *out);
 /* per column of the last emg_solve_block(_dev): the relative residual
  * ||b - A x0|| / ||b|| of the start it used (1 for a zero start, also where
  * a guess was worse than zero and was dropped) */
