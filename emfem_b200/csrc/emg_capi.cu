@@ -1339,17 +1339,22 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
     cudaEvent_t ph = nullptr;
     if (pf.phases) pf.begin("phase_ams", c.stream, 0, &ph);
     (void)r_;  // w.f_in holds (float) r_: the FCG update writes it
+    (void)z_;  // z = f_out + G gphi is formed inside the FCG's passes
     w.bams32.apply(w.f_in.p, w.f_out.p, c.stream);
-    add_gradient_f2d(n, K2, c.edges.p, w.f_out.p, w.bams32.gphi(), z_, c.stream);
     if (pf.phases) pf.end("phase_ams", c.stream, ph);
   };
+  Fcg<double>::ZSplit zsplit{c.edges.p, nullptr, nullptr};
   auto pc = [&](const double *v, double *z) {
     KernelProfiler &pf = profiler();
     cudaEvent_t ph = nullptr;
     if (pf.phases) pf.begin("phase_fcg", c.stream, 0, &ph);
-    if (fp32)
+    if (fp32) {
+      if (w.fcg64.mmax > 4) fail(EMG_ERR_OPTION, "-emg_block_fcg_mmax above 4 with the FP32 preconditioner");
+      zsplit.x = w.f_out.p;
+      zsplit.phi = w.bams32.gphi();
       w.fcg64.solve_with(n, K2, pc32, opB64, v, z, c.opt.block_inner_rtol, c.opt.block_inner_max_it, c.stream,
-                         w.f_in.p);
+                         w.f_in.p, &zsplit);
+    }
     else w.fcg64.solve(w.bams64, v, z, c.opt.block_inner_rtol, c.opt.block_inner_max_it, c.stream);
     if (pf.phases) pf.end("phase_fcg", c.stream, ph);
   };

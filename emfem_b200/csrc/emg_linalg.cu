@@ -443,6 +443,68 @@ void add_gradient_f2d(int ne, int K, const int *edges, const float *x, const flo
   EMG_LAUNCH_CHECK();
 }
 
+// z = x + G phi formed on the fly (FP64 from the FP32 AMS output and its
+// gradient potential), never stored: the FCG needs z only for its dot
+// products with the previous B-products and for the new direction
+__device__ __forceinline__ double zsplit_at(long i, int K, const int *__restrict__ edges,
+                                            const float *__restrict__ x, const float *__restrict__ phi) {
+  const long e = i / K;
+  const int c = (int)(i % K);
+  const int v0 = __ldg(edges + 2 * e), v1 = __ldg(edges + 2 * e + 1);
+  return (double)x[i] + ((double)__ldg(phi + (long)v1 * K + c) - (double)__ldg(phi + (long)v0 * K + c));
+}
+
+__global__ void __launch_bounds__(256) zsplit_dots_kernel(long total, int K, const int *__restrict__ edges,
+                                                          const float *__restrict__ x, const float *__restrict__ phi,
+                                                          int nprev, DevPtrs4 S, double *__restrict__ out) {
+  __shared__ double sh[4][256];
+  double acc[4] = {0, 0, 0, 0};
+  for (long i = blockIdx.x * 256L + threadIdx.x; i < total; i += (long)gridDim.x * 256) {
+    const double z = zsplit_at(i, K, edges, x, phi);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (j < nprev) acc[j] += z * S.p[j][i];
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) sh[j][threadIdx.x] = acc[j];
+  __syncthreads();
+  for (int st = 128; st >= K; st >>= 1) {
+    if ((int)threadIdx.x < st)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) sh[j][threadIdx.x] += sh[j][threadIdx.x + st];
+    __syncthreads();
+  }
+  if ((int)threadIdx.x < K)
+    for (int j = 0; j < nprev; ++j) atomicAdd(out + j * K + threadIdx.x, sh[j][threadIdx.x]);
+}
+
+__global__ void zsplit_direction_kernel(long total, int K, const int *__restrict__ edges, const float *__restrict__ x,
+                                        const float *__restrict__ phi, int nprev, double *const *Pj,
+                                        const double *__restrict__ beta, double *__restrict__ p) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int c = (int)(i % K);
+  double v = zsplit_at(i, K, edges, x, phi);
+  for (int j = 0; j < nprev; ++j) v -= beta[j * K + c] * Pj[j][i];
+  p[i] = v;
+}
+
+void zsplit_dots(int n, int K, const int *edges, const float *x, const float *phi, int nprev, const DevPtrs4 &S,
+                 double *out, cudaStream_t s) {
+  const long total = (long)n * K;
+  if (nprev < 1 || nprev > 4) fail(EMG_ERR_ARG, "zsplit_dots: 1..4 previous directions");
+  zsplit_dots_kernel<<<red_grid(total), 256, 0, s>>>(total, K, edges, x, phi, nprev, S, out);
+  EMG_LAUNCH_CHECK();
+}
+
+void zsplit_direction(int n, int K, const int *edges, const float *x, const float *phi, int nprev,
+                      double *const *Pj, const double *beta, double *p, cudaStream_t s) {
+  const long total = (long)n * K;
+  zsplit_direction_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, edges, x, phi, nprev, Pj, beta,
+                                                                          p);
+  EMG_LAUNCH_CHECK();
+}
+
 template <typename T>
 void fill_zero(long count, T *a, cudaStream_t s) {
   if (count) EMG_CUDA(cudaMemsetAsync(a, 0, count * sizeof(T), s));

@@ -71,6 +71,16 @@ void cvt_f2d(long count, const float *a, double *b, cudaStream_t s);
 void add_gradient_f2d(int ne, int K, const int *edges, const float *x, const float *phi, double *z, cudaStream_t s);
 template <typename T>
 void fill_zero(long count, T *a, cudaStream_t s);
+// FCG steps with z = x + G phi formed on the fly (FP32 AMS output x, FP32
+// gradient potential phi): out[j*K+c] += (z_c, S_j,c) for j < nprev (<= 4),
+// and p = z - sum_j beta[j*K+c] P_j
+struct DevPtrs4 {
+  const double *p[4];
+};
+void zsplit_dots(int n, int K, const int *edges, const float *x, const float *phi, int nprev, const DevPtrs4 &S,
+                 double *out, cudaStream_t s);
+void zsplit_direction(int n, int K, const int *edges, const float *x, const float *phi, int nprev,
+                      double *const *Pj, const double *beta, double *p, cudaStream_t s);
 
 // AMS transfers between edges and vertices for K columns.
 //   sp == 0: gradient G (row e: -1 at edges[e][0], +1 at edges[e][1])

@@ -933,8 +933,9 @@ __global__ void fcg_status_kernel(int K, const double *__restrict__ rn, const do
 template <typename T>
 int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> &pc,
                        const std::function<void(const T *, T *)> &opB, const T *b, T *x, double rtol, int maxit,
-                       cudaStream_t s, float *r32) {
+                       cudaStream_t s, float *r32, const ZSplit *zs) {
   K = Kc;
+  if (zs && (sizeof(T) != 8 || mmax > 4)) fail(EMG_ERR_STATE, "split z needs FP64 recurrences and at most 4 directions");
   const size_t N = (size_t)n * K;
   if (mmax < 1) mmax = 1;
   if (K > 1024) fail(EMG_ERR_ARG, "batched FCG supports at most 1024 columns");
@@ -988,7 +989,25 @@ int Fcg<T>::solve_with(int n, int Kc, const std::function<void(const T *, T *)> 
   int nprev = 0, head = 0, it = 0;
   for (it = 0; it < maxit; ++it) {
     pc(r.p, z.p);
-    if (nprev > 0) {
+    if (zs) {
+      // z = x + G phi only inside these two passes
+      if (nprev > 0) {
+        EMG_CUDA(cudaMemsetAsync(dots.p, 0, sizeof(double) * nprev * K, s));
+        DevPtrs4 Sj{{nullptr, nullptr, nullptr, nullptr}};
+        for (int j = 0; j < nprev; ++j) {
+          const int sl = (head - nprev + j + mmax) % mmax;
+          Sj.p[j] = reinterpret_cast<const double *>(S[sl].p);
+          EMG_CUDA(cudaMemcpyAsync(eord.p + (size_t)j * K, eta.p + (size_t)sl * K, sizeof(double) * K,
+                                   cudaMemcpyDeviceToDevice, s));
+        }
+        zsplit_dots(n, K, zs->edges, zs->x, zs->phi, nprev, Sj, dots.p, s);
+        fcg_beta_kernel<<<(nprev * K + 127) / 128, 128, 0, s>>>(K, nprev, dots.p, eord.p, act.p, beta.p);
+        EMG_LAUNCH_CHECK();
+      }
+      zsplit_direction(n, K, zs->edges, zs->x, zs->phi, nprev,
+                       reinterpret_cast<double *const *>(ptrs.p + ((size_t)head * (mmax + 1) + nprev) * mmax),
+                       beta.p, reinterpret_cast<double *>(P[head].p), s);
+    } else if (nprev > 0) {
       EMG_CUDA(cudaMemsetAsync(dots.p, 0, sizeof(double) * nprev * K, s));
       for (int j = 0; j < nprev; ++j) {
         const int sl = (head - nprev + j + mmax) % mmax;

@@ -213,9 +213,16 @@ struct Fcg {
   // generic form: pc(r, z) applies the preconditioner, opB(p, s) the operator;
   // n rows, K columns
   // r32: when given, kept equal to (float) r for an FP32 preconditioner
+  // zs: the preconditioner leaves z split as x + G phi in FP32 (zs->x, zs->phi
+  // over the edges zs->edges) instead of writing z; the dot products and the
+  // direction then form z on the fly
+  struct ZSplit {
+    const int *edges;
+    const float *x, *phi;
+  };
   int solve_with(int n, int Kc, const std::function<void(const T *, T *)> &pc,
                  const std::function<void(const T *, T *)> &opB, const T *b, T *x, double rtol, int maxit,
-                 cudaStream_t s, float *r32 = nullptr);
+                 cudaStream_t s, float *r32 = nullptr, const ZSplit *zs = nullptr);
 };
 
 struct SolveStats {
