@@ -223,6 +223,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_fused_blocks_per_sm") o.fused_bps = geti(k, v);
     else if (key == "emg_fused_rows") o.fused_rows = geti(k, v);
     else if (key == "emg_gpu_amg") o.gpu_amg = v.empty() ? 1 : getb(v);
+    else if (key == "emg_block_fp64_fallback") o.block_fp64_fallback = v.empty() ? 1 : getb(v);
     else if (key == "emg_fused_wait_ms") o.fused_wait_ms = getr(k, v);
     else if (key == "emg_fused_test_withhold") o.fused_test_withhold = geti(k, v);
     else if (key == "emg_pi_coupled") o.pi_coupled = v.empty() ? 1 : getb(v);
@@ -633,6 +634,7 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_fused_blocks_per_sm") *value = o.fused_bps;
   else if (k == "emg_fused_rows") *value = o.fused_rows;
   else if (k == "emg_gpu_amg") *value = o.gpu_amg;
+  else if (k == "emg_block_fp64_fallback") *value = o.block_fp64_fallback;
   else if (k == "emg_fused_wait_ms") *value = o.fused_wait_ms;
   else if (k == "emg_fused_test_withhold") *value = o.fused_test_withhold;
   else if (k == "emg_pi_coupled") *value = o.pi_coupled;
@@ -928,6 +930,7 @@ int emg_solve_linear_system(emg_context *c, int target, const double *s_re, cons
   w.vec_a.upload(bi, c->stream);
   w.gm.k = 1;
   w.gm.restart = c->opt.gmres_restart;
+  w.gm.stall_factor = 0.0;  // the reference's FGMRES runs to rtol or max_it
   w.gm.omega.upload(&c->omega, 1, c->stream);
   w.fcg64.mmax = c->opt.fcg_mmax;
   w.fcg64.check_every = 1;
@@ -1294,6 +1297,9 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
   EMG_LAUNCH_CHECK();
   w.gm.k = k;
   w.gm.restart = o.restart > 0 ? o.restart : c.opt.gmres_restart;
+  // with the FP64 fallback behind it, an FP32 column that stops making
+  // progress (less than 2x over a restart cycle) is handed over early
+  w.gm.stall_factor = (fp32 && c.opt.block_fp64_fallback) ? 0.5 : 0.0;
   w.gm.omega.upload(om, c.stream);
   w.fcg64.mmax = w.fcg32.mmax = c.opt.block_fcg_mmax;
   w.fcg64.check_every = w.fcg32.check_every = c.opt.block_fcg_check_every;
@@ -1375,6 +1381,31 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
     for (int j = 0; j < k; ++j) fill_info(&infos[j], st, inner, j);
   c.kernel_ms["solve_block"] = st.seconds * 1e3;
   c.block_initial_res = st.initial_res;
+  // a column the FP32 preconditioner could not carry to rtol within max_it
+  // (stagnation at low frequency) is finished with the FP64 preconditioner,
+  // starting from where it stopped; converged columns pass through at the
+  // cost of one residual
+  bool all_conv = true;
+  for (int j = 0; j < k; ++j) all_conv = all_conv && st.converged[j];
+  if (fp32 && !all_conv && c.opt.block_fp64_fallback) {
+    emg_block_opts o2 = o;
+    o2.inner_fp32 = 0;
+    o2.use_guess = 1;
+    std::vector<emg_solve_info> inf2(k);
+    std::vector<double> r0 = st.initial_res;
+    const double s1 = st.seconds;
+    solve_block_pow2(c, k, freqs, rhs_dev, x_dev, o2, inf2.data());
+    if (infos)
+      for (int j = 0; j < k; ++j) {
+        infos[j].outer_its += inf2[j].outer_its;
+        infos[j].inner_its += inf2[j].inner_its;
+        infos[j].reason = inf2[j].reason;
+        infos[j].true_rel_res = inf2[j].true_rel_res;
+        infos[j].seconds += inf2[j].seconds;
+      }
+    c.kernel_ms["solve_block"] += s1 * 1e3;
+    c.block_initial_res = r0;
+  }
 }
 
 // Any number of columns: blocks of at most kMaxBlock columns solved one after

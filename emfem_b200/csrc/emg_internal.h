@@ -170,6 +170,7 @@ struct Options {
   int amg_relax_times = 1;
   int smoother_cheb = 1;  // degree-2 Chebyshev (1) or l1-Jacobi (0) in AMS and AMG
   int gpu_amg = 1;        // nodal AMG setup on the device (1) or on the host (0)
+  int block_fp64_fallback = 1;  // batched path: columns the FP32 AMS leaves unconverged finish in FP64
   // emg_*
   int inner_fp32 = 0;
   int graphs = 1;

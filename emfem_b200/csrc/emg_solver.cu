@@ -1105,14 +1105,20 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double zabs(double2 a) { return hypot(a.x, a.y); }
 
-// start of a restart cycle: nrm2[c] = ||b - A x||^2
-__global__ void gm_start_kernel(int K, int J, const double *__restrict__ nrm2, double rtol, GmDev st) {
+// start of a restart cycle: nrm2[c] = ||b - A x||^2.  stall > 0: a column
+// whose residual fell by less than that factor over the last cycle stops
+// iterating (it leaves unconverged, for a caller with a stronger
+// preconditioner to finish)
+__global__ void gm_start_kernel(int K, int J, const double *__restrict__ nrm2, double rtol, double stall,
+                                double *__restrict__ prev, GmDev st) {
   const int c = threadIdx.x;
   int act = 0;
   if (c < K) {
     const double beta = sqrt(nrm2[c]);
     if (!isfinite(beta)) atomicCAS(st.status + 1, 0, c + 1);
     if (beta <= rtol * st.bnorm[c]) st.conv[c] = 1;
+    if (stall > 0 && prev[c] > 0 && beta > stall * prev[c]) st.conv[c] = 1;
+    prev[c] = beta;
     const bool cv = st.conv[c] != 0 || !isfinite(beta);
     for (int i = 0; i <= J; ++i) st.g[(long)c * (J + 1) + i] = make_double2(0, 0);
     st.g[(long)c * (J + 1)] = make_double2(cv ? 0.0 : beta, 0.0);
@@ -1243,6 +1249,8 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   gs.bnorm = bnd.p;
   gs.scale = scale.p;
   ints.zero(s);
+  prevb.alloc(k);
+  prevb.zero(s);
   if (!use_guess) fill_zero<double>((long)N2, x, s);
   cudaEvent_t e0, e1;
   EMG_CUDA(cudaEventCreate(&e0));
@@ -1299,7 +1307,7 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
     spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, r.p, true, real_form, s);
     nrm.zero(s);
     cnorm2(n, k, r.p, nrm.p, s);
-    gm_start_kernel<<<1, 1024, 0, s>>>(k, J, nrm.p, rtol, gs);
+    gm_start_kernel<<<1, 1024, 0, s>>>(k, J, nrm.p, rtol, stall_factor, prevb.p, gs);
     EMG_LAUNCH_CHECK();
     if (read_status() == 0) break;
     cscale(n, k, r.p, scale.p, V.p, s);

@@ -246,6 +246,8 @@ struct Fgmres {
   DBuf<double> bnd, Hd, csd, snd, gd;  // per-column norms, Hessenberg, rotations, rotated rhs (device)
   DBuf<int> ints;                      // done, jc, its, conv per column; two status words
   PinnedWord h_status;
+  DBuf<double> prevb;                  // residual norm at the previous restart, per column
+  double stall_factor = 0;             // > 0: stop a column whose residual fell less than this over a cycle
   int solve(Context &c, const double *b, double *x, bool use_guess, double rtol, int maxit, bool real_form,
             const std::function<void(const double *, double *)> &precond, SolveStats &st);
 };
