@@ -98,14 +98,37 @@ struct FusedOp {
   SpmmArgs a;
 };
 
-// Row epilogue shared by the SpMM kernels: combines the row product acc
-// (columns cb*V .. cb*V+V-1 of row `row`) with the vectors the mode needs and
-// stores the result row.
+// Row epilogue shared by the SpMM kernels, in two halves: epi_load reads
+// the row vectors the mode needs (b, x, r, y and the l1 sums; none of them
+// depends on the row product, so the kernels issue these loads before the
+// gathers and they overlap), epi_store combines them with the row product
+// acc (columns cb*V .. cb*V+V-1 of row `row`) and stores the results.
+template <typename T, int V>
+struct EpiIn {
+  T b[V], x[V], r[V], y[V];
+  T dc, dm;
+};
+
 template <typename T, int K, int V>
-__device__ __forceinline__ void spmm_epilogue(const SpmmArgs &a, int row, int cb, const T (&acc)[V], const T (&w)[V],
-                                              bool two) {
+__device__ __forceinline__ void epi_load(const SpmmArgs &a, int row, int cb, bool two, EpiIn<T, V> &e) {
   const long o = (long)row * K + cb * V;
   const T *__restrict__ x = static_cast<const T *>(a.x);
+  T *y = static_cast<T *>(a.y);
+  const int mode = a.mode;
+  if (mode == SPMM_RES || mode == SPMM_JAC || mode == SPMM_CHEB1) ldv<T, V>(static_cast<const T *>(a.b) + o, e.b);
+  if (mode == SPMM_JAC || mode == SPMM_CHEB1 || mode == SPMM_CHEB2) ldv<T, V>(x + o, e.x);
+  if (mode == SPMM_CHEB2) ldv<T, V>(static_cast<const T *>(a.r) + o, e.r);
+  if (mode == SPMM_ADD || mode == SPMM_CHEB2) ldv_plain<T, V>(y + o, e.y);
+  if (mode == SPMM_JAC || mode == SPMM_CHEB1 || mode == SPMM_CHEB2) {
+    e.dc = __ldg(static_cast<const T *>(a.l1c) + row);
+    e.dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+  }
+}
+
+template <typename T, int K, int V>
+__device__ __forceinline__ void epi_store(const SpmmArgs &a, int row, int cb, const T (&acc)[V], const T (&w)[V],
+                                          bool two, const EpiIn<T, V> &e) {
+  const long o = (long)row * K + cb * V;
   T *y = static_cast<T *>(a.y);
   T out[V];
   switch (a.mode) {
@@ -113,65 +136,50 @@ __device__ __forceinline__ void spmm_epilogue(const SpmmArgs &a, int row, int cb
 #pragma unroll
     for (int i = 0; i < V; ++i) out[i] = acc[i];
     break;
-  case SPMM_RES: {
-    T bv[V];
-    ldv<T, V>(static_cast<const T *>(a.b) + o, bv);
+  case SPMM_RES:
 #pragma unroll
-    for (int i = 0; i < V; ++i) out[i] = bv[i] - acc[i];
+    for (int i = 0; i < V; ++i) out[i] = e.b[i] - acc[i];
     break;
-  }
-  case SPMM_JAC: {
-    T bv[V], xo[V];
-    ldv<T, V>(static_cast<const T *>(a.b) + o, bv);
-    ldv<T, V>(x + o, xo);
-    const T dc = __ldg(static_cast<const T *>(a.l1c) + row);
-    const T dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+  case SPMM_JAC:
 #pragma unroll
     for (int i = 0; i < V; ++i) {
-      T d = two ? dc + w[i] * dm : dc;
-      out[i] = xo[i] + (T)a.relax_w * (bv[i] - acc[i]) / d;
+      T d = two ? e.dc + w[i] * e.dm : e.dc;
+      out[i] = e.x[i] + (T)a.relax_w * (e.b[i] - acc[i]) / d;
     }
     break;
-  }
-  case SPMM_ADD: {
-    T yo[V];
-    ldv_plain<T, V>(y + o, yo);
+  case SPMM_ADD:
 #pragma unroll
-    for (int i = 0; i < V; ++i) out[i] = yo[i] + acc[i];
+    for (int i = 0; i < V; ++i) out[i] = e.y[i] + acc[i];
     break;
-  }
   case SPMM_CHEB1: {
-    T bv[V], xo[V], rr[V], dd[V];
-    ldv<T, V>(static_cast<const T *>(a.b) + o, bv);
-    ldv<T, V>(x + o, xo);
-    const T dc = __ldg(static_cast<const T *>(a.l1c) + row);
-    const T dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+    T rr[V], dd[V];
 #pragma unroll
     for (int i = 0; i < V; ++i) {
-      T dg = two ? dc + w[i] * dm : dc;
-      rr[i] = bv[i] - acc[i];
+      T dg = two ? e.dc + w[i] * e.dm : e.dc;
+      rr[i] = e.b[i] - acc[i];
       dd[i] = (T)a.c1 * rr[i] / dg;
-      out[i] = xo[i] + dd[i];
+      out[i] = e.x[i] + dd[i];
     }
     stv<T, V>(static_cast<T *>(a.r) + o, rr);
     stv<T, V>(static_cast<T *>(a.d) + o, dd);
     break;
   }
-  default: {  // SPMM_CHEB2: x is d (gathered), r holds the residual
-    T rr[V], dd[V], yo[V];
-    ldv<T, V>(static_cast<const T *>(a.r) + o, rr);
-    ldv<T, V>(x + o, dd);
-    ldv_plain<T, V>(y + o, yo);
-    const T dc = __ldg(static_cast<const T *>(a.l1c) + row);
-    const T dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+  default:  // SPMM_CHEB2: x is d (gathered), r holds the residual
 #pragma unroll
     for (int i = 0; i < V; ++i) {
-      T dg = two ? dc + w[i] * dm : dc;
-      out[i] = yo[i] + (T)a.c1 * dd[i] + (T)a.c2 * (rr[i] - acc[i]) / dg;
+      T dg = two ? e.dc + w[i] * e.dm : e.dc;
+      out[i] = e.y[i] + (T)a.c1 * e.x[i] + (T)a.c2 * (e.r[i] - acc[i]) / dg;
     }
   }
-  }
   stv<T, V>(y + o, out);
+}
+
+template <typename T, int K, int V>
+__device__ __forceinline__ void spmm_epilogue(const SpmmArgs &a, int row, int cb, const T (&acc)[V], const T (&w)[V],
+                                              bool two) {
+  EpiIn<T, V> e;
+  epi_load<T, K, V>(a, row, cb, two, e);
+  epi_store<T, K, V>(a, row, cb, acc, w, two, e);
 }
 
 template <typename T, int K, int V, int NL>
@@ -196,6 +204,8 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
 #pragma unroll
   for (int i = 0; i < V; ++i) w[i] = two ? (T)__ldg(a.omega + cb * V + i) : T(0);
   const bool valid = row < a.n;
+  EpiIn<T, V> epi;
+  if (valid && sl == 0) epi_load<T, K, V>(a, row, cb, two, epi);
   if (valid) {
     const int kb = __ldg(a.rp + row), ke = __ldg(a.rp + row + 1);
     // U nonzeros per lane per round: all index/value loads of the round are
@@ -234,7 +244,7 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
 #pragma unroll
     for (int i = 0; i < V; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
   if (!valid || sl != 0) return;
-  spmm_epilogue<T, K, V>(a, row, cb, acc, w, two);
+  epi_store<T, K, V>(a, row, cb, acc, w, two, epi);
 }
 
 // Row-group SpMM: G = K / V lanes serve one row (lane j owns column block j),
@@ -266,6 +276,8 @@ __global__ void __launch_bounds__(256) spmm_rows_kernel(SpmmArgs a) {
   }
   const int kb = valid ? __ldg(a.rp + row) : 0;
   const int len = valid ? __ldg(a.rp + row + 1) - kb : 0;
+  EpiIn<T, V> epi;
+  if (valid) epi_load<T, K, V>(a, row, j, two, epi);
   int maxlen = len;
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, off));
@@ -296,7 +308,7 @@ __global__ void __launch_bounds__(256) spmm_rows_kernel(SpmmArgs a) {
     }
   }
   if (!valid) return;
-  spmm_epilogue<T, K, V>(a, row, j, acc, w, two);
+  epi_store<T, K, V>(a, row, j, acc, w, two, epi);
 }
 
 // Row tiles with their own column lists: tile t covers rows [t R, t R + R);
