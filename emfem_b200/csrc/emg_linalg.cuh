@@ -282,10 +282,12 @@ __global__ void __launch_bounds__(256) spmm_rows_kernel(SpmmArgs a) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, off));
   for (int c0 = 0; c0 < maxlen; c0 += G) {
+    // the index and value streams are read once: streaming loads keep them
+    // out of L1, which the x gathers reuse
     const bool ok = c0 + j < len;
-    const int cj = ok ? __ldg(a.ci + kb + c0 + j) : 0;
-    const T cc = ok ? __ldg(vc + kb + c0 + j) : T(0);
-    const T cm = (ok && two) ? __ldg(vm + kb + c0 + j) : T(0);
+    const int cj = ok ? __ldcs(a.ci + kb + c0 + j) : 0;
+    const T cc = ok ? __ldcs(vc + kb + c0 + j) : T(0);
+    const T cm = (ok && two) ? __ldcs(vm + kb + c0 + j) : T(0);
 #pragma unroll
     for (int t0 = 0; t0 < G; t0 += B) {
       T xv[B][V], ct[B], mt[B];
