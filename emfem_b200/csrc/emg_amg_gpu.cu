@@ -84,6 +84,7 @@ int scan_excl(int *a, long n, cudaStream_t s) {
   int tot = 0;
   EMG_CUDA(cudaMemcpyAsync(&tot, a + n, sizeof(int), cudaMemcpyDeviceToHost, s));
   EMG_CUDA(cudaStreamSynchronize(s));
+  if (tot < 0) fail(EMG_ERR_USER, "AMG setup: a prefix sum overflowed (%d)", tot);
   return tot;
 }
 
@@ -502,6 +503,7 @@ void gcsr_galerkin(const GCsr &R, const GCsr &A, const GCsr &P, GCsr &C, cudaStr
   C.n = R.n;
   C.m = P.m;
   C.rp.alloc((size_t)C.n + 1);
+  C.rp.zero(s);
   RapArgs a{};
   a.nc = C.n;
   a.rrp = R.rp.p;
@@ -645,6 +647,7 @@ void amg_build_gpu(GCsr A, double w_ref, const AmgParams &prm, std::vector<GpuLe
     P.n = n;
     P.m = nc;
     P.rp.alloc((size_t)n + 1);
+    P.rp.zero(s);
     InterpArgs ia{};
     ia.n = n;
     ia.pmax = std::min(prm.pmax, 8);
@@ -659,7 +662,7 @@ void amg_build_gpu(GCsr A, double w_ref, const AmgParams &prm, std::vector<GpuLe
     ia.cf = cf.p;
     ia.cidx = cidx.p;
     ia.cnt = P.rp.p;
-    interp_kernel<<<nblk(n), 128, 0, s>>>(ia);
+    interp_kernel<<<nblk(n, 128), 128, 0, s>>>(ia);
     EMG_LAUNCH_CHECK();
     P.nnz = scan_excl(P.rp.p, n, s);
     P.ci.alloc(std::max<size_t>(P.nnz, 1));
@@ -668,7 +671,7 @@ void amg_build_gpu(GCsr A, double w_ref, const AmgParams &prm, std::vector<GpuLe
     ia.prp = P.rp.p;
     ia.pci = P.ci.p;
     ia.pv = P.vc.p;
-    interp_kernel<<<nblk(n), 128, 0, s>>>(ia);
+    interp_kernel<<<nblk(n, 128), 128, 0, s>>>(ia);
     EMG_LAUNCH_CHECK();
     DBuf<int> fc;
     if (fn.p) {
