@@ -183,6 +183,8 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
   return x;
 }
 
+constexpr float kTargetClamp = 2.0f;
+
 struct KArgs {
   const unsigned char *img;  // packed BF16 weight image (IMG_BYTES)
   const float *bias;         // 4 x 64 (b1, b2, b3, b4 padded)
@@ -253,9 +255,12 @@ __device__ __forceinline__ void sample_features(const KArgs &a, long s, bool val
   b0 = (1.f - p.tau) * f[0] + p.tau * f[2];
   b1 = (1.f - p.tau) * f[1] + p.tau * f[3];
   if (a.mode == 2) {
+    // corrections larger than a few neighbour magnitudes are outliers
+    // (edges where both neighbours nearly vanish): clamped, so that a few of
+    // them do not dominate the squared loss
     const double2 et = a.xs[(long)e * a.ks + p.tcol];
-    t0 = (float)(et.x * inv) - b0;
-    t1 = (float)(et.y * inv) - b1;
+    t0 = fminf(fmaxf((float)(et.x * inv) - b0, -kTargetClamp), kTargetClamp);
+    t1 = fminf(fmaxf((float)(et.y * inv) - b1, -kTargetClamp), kTargetClamp);
   }
 }
 

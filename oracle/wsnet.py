@@ -132,8 +132,8 @@ def features(stat, xs, spec, edges, with_target):
     tgt = np.zeros((n, 2), dtype=np.float32)
     if with_target:
         et = xs[edges, spec["tcol"]]
-        tgt[:, 0] = (et.real * inv).astype(np.float32) - base[:, 0]
-        tgt[:, 1] = (et.imag * inv).astype(np.float32) - base[:, 1]
+        tgt[:, 0] = np.clip((et.real * inv).astype(np.float32) - base[:, 0], -2.0, 2.0)
+        tgt[:, 1] = np.clip((et.imag * inv).astype(np.float32) - base[:, 1], -2.0, 2.0)
         tgt[~ok] = 0
     return f, base, np.where(ok, sc, 0.0), tgt
 
