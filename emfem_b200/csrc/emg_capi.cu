@@ -224,6 +224,8 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_fused_rows") o.fused_rows = geti(k, v);
     else if (key == "emg_gpu_amg") o.gpu_amg = v.empty() ? 1 : getb(v);
     else if (key == "emg_block_fp64_fallback") o.block_fp64_fallback = v.empty() ? 1 : getb(v);
+    else if (key == "emg_block_fp32_rtol_factor") o.block_fp32_rtol_factor = getr(k, v);
+    else if (key == "emg_block_fp64_below") o.block_fp64_below_hz = getr(k, v);
     else if (key == "emg_fused_wait_ms") o.fused_wait_ms = getr(k, v);
     else if (key == "emg_fused_test_withhold") o.fused_test_withhold = geti(k, v);
     else if (key == "emg_pi_coupled") o.pi_coupled = v.empty() ? 1 : getb(v);
@@ -239,6 +241,8 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
   }
   if (o.gmres_restart < 1 || o.gmres_restart > 32) fail(EMG_ERR_OPTION, "A_ksp_gmres_restart must be in [1, 32]");
   if (o.block_fcg_check_every < 1) fail(EMG_ERR_OPTION, "-emg_block_fcg_check_every must be >= 1");
+  if (!(o.block_fp32_rtol_factor > 0 && o.block_fp32_rtol_factor <= 1))
+    fail(EMG_ERR_OPTION, "-emg_block_fp32_rtol_factor must be in (0, 1]");
   if (o.fcg_mmax < 1 || o.fcg_mmax > 30 || o.block_fcg_mmax < 1 || o.block_fcg_mmax > 30)
     fail(EMG_ERR_OPTION, "FCG truncation lengths must be in [1, 30]");
   if (o.ams_relax_times < 1 || o.amg_relax_times < 1) fail(EMG_ERR_OPTION, "relax times must be >= 1");
@@ -635,6 +639,8 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_fused_rows") *value = o.fused_rows;
   else if (k == "emg_gpu_amg") *value = o.gpu_amg;
   else if (k == "emg_block_fp64_fallback") *value = o.block_fp64_fallback;
+  else if (k == "emg_block_fp32_rtol_factor") *value = o.block_fp32_rtol_factor;
+  else if (k == "emg_block_fp64_below") *value = o.block_fp64_below_hz;
   else if (k == "emg_fused_wait_ms") *value = o.fused_wait_ms;
   else if (k == "emg_fused_test_withhold") *value = o.fused_test_withhold;
   else if (k == "emg_pi_coupled") *value = o.pi_coupled;
@@ -1369,8 +1375,10 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
     KernelProfiler &pf = profiler();
     cudaEvent_t ph = nullptr;
     if (pf.phases) pf.begin("phase_fgmres", c.stream, 0, &ph);
-    w.gm.solve(c, w.vec_a.p, x_dev, o.use_guess != 0, o.rtol > 0 ? o.rtol : c.opt.e_rtol,
-               o.max_it > 0 ? o.max_it : c.opt.K_max_it, false, pc, st);
+    // FP32-preconditioned columns iterate further (rounding noise of the
+    // FP32 AMS in the gradient space of the air is invisible to the residual)
+    const double rtol = (o.rtol > 0 ? o.rtol : c.opt.e_rtol) * (fp32 ? c.opt.block_fp32_rtol_factor : 1.0);
+    w.gm.solve(c, w.vec_a.p, x_dev, o.use_guess != 0, rtol, o.max_it > 0 ? o.max_it : c.opt.K_max_it, false, pc, st);
     if (pf.phases) pf.end("phase_fgmres", c.stream, ph);
   }
   EMG_CUDA(cudaStreamSynchronize(c.stream));
@@ -1408,50 +1416,99 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
   }
 }
 
-// Any number of columns: blocks of at most kMaxBlock columns solved one after
-// another; a block whose width is not a power of two is padded with zero
-// right-hand sides (they converge at once and stay inactive in the inner
-// solves) at its last column's frequency.
-static void solve_block_dev(Context &c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
-                            const emg_block_opts &o, emg_solve_info *infos) {
+// columns src[0..m) of an n x k complex block into an n x kb block (zero
+// columns beyond m), and back
+struct ColMap {
+  int m;
+  int src[32];
+};
+
+__global__ void gather_cols_kernel(long n, int k, int kb, ColMap cm, const double2 *__restrict__ in,
+                                   double2 *__restrict__ out) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n * kb) return;
+  const long i = t / kb;
+  const int j = (int)(t - i * kb);
+  out[t] = j < cm.m ? in[i * k + cm.src[j]] : make_double2(0.0, 0.0);
+}
+
+__global__ void scatter_cols_kernel(long n, int k, int kb, ColMap cm, const double2 *__restrict__ in,
+                                    double2 *__restrict__ out) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n * cm.m) return;
+  const long i = t / cm.m;
+  const int j = (int)(t - i * cm.m);
+  out[i * k + cm.src[j]] = in[i * kb + j];
+}
+
+// The columns idx of an n x k block, in blocks of at most kMaxBlock columns
+// solved one after another; a block whose width is not a power of two is
+// padded with zero right-hand sides (they converge at once and stay inactive
+// in the inner solves) at its last column's frequency.
+static void solve_block_subset(Context &c, const std::vector<int> &idx, int k, const double *freqs,
+                               const double *rhs_dev, double *x_dev, const emg_block_opts &o,
+                               emg_solve_info *infos, double &total_s, std::vector<double> &r0) {
   constexpr int kMaxBlock = 32;
-  need(k >= 1, EMG_ERR_ARG, "block width k must be positive");
+  const int m = (int)idx.size();
   int kp = 1;
-  while (kp < k) kp <<= 1;
-  if (k <= kMaxBlock && kp == k) {
+  while (kp < m) kp <<= 1;
+  if (m == k && kp == k && k <= kMaxBlock) {  // the whole block as it lies
     solve_block_pow2(c, k, freqs, rhs_dev, x_dev, o, infos);
+    total_s += c.kernel_ms["solve_block"] * 1e-3;
+    for (int j = 0; j < k && j < (int)c.block_initial_res.size(); ++j) r0[j] = c.block_initial_res[j];
     return;
   }
   Workspace &w = *c.ws;
-  const size_t n = (size_t)c.ne;
-  double total_s = 0;
-  std::vector<double> r0(k, 1.0);
-  for (int j0 = 0; j0 < k; j0 += kMaxBlock) {
-    const int kc = std::min(kMaxBlock, k - j0);
+  const long n = c.ne;
+  for (int j0 = 0; j0 < m; j0 += kMaxBlock) {
+    ColMap cm;
+    cm.m = std::min(kMaxBlock, m - j0);
     int kb = 1;
-    while (kb < kc) kb <<= 1;
-    std::vector<double> f(kb, freqs[j0 + kc - 1]);
-    std::copy(freqs + j0, freqs + j0 + kc, f.begin());
-    w.blk_rhs.alloc(n * kb * 2);
-    w.blk_x.alloc(n * kb * 2);
-    const size_t dst_pitch = (size_t)kb * 16, src_pitch = (size_t)k * 16, width = (size_t)kc * 16;
-    if (kb != kc) w.blk_rhs.zero(c.stream);
-    EMG_CUDA(cudaMemcpy2DAsync(w.blk_rhs.p, dst_pitch, rhs_dev + (size_t)j0 * 2, src_pitch, width, n,
-                               cudaMemcpyDeviceToDevice, c.stream));
+    while (kb < cm.m) kb <<= 1;
+    std::vector<double> f(kb, freqs[idx[j0 + cm.m - 1]]);
+    for (int j = 0; j < cm.m; ++j) {
+      cm.src[j] = idx[j0 + j];
+      f[j] = freqs[cm.src[j]];
+    }
+    w.blk_rhs.alloc((size_t)n * kb * 2);
+    w.blk_x.alloc((size_t)n * kb * 2);
+    const unsigned gb = (unsigned)((n * kb + 255) / 256), gs = (unsigned)((n * cm.m + 255) / 256);
+    gather_cols_kernel<<<gb, 256, 0, c.stream>>>(n, k, kb, cm, (const double2 *)rhs_dev, (double2 *)w.blk_rhs.p);
+    EMG_LAUNCH_CHECK();
     if (o.use_guess) {
-      if (kb != kc) w.blk_x.zero(c.stream);
-      EMG_CUDA(cudaMemcpy2DAsync(w.blk_x.p, dst_pitch, x_dev + (size_t)j0 * 2, src_pitch, width, n,
-                                 cudaMemcpyDeviceToDevice, c.stream));
+      gather_cols_kernel<<<gb, 256, 0, c.stream>>>(n, k, kb, cm, (const double2 *)x_dev, (double2 *)w.blk_x.p);
+      EMG_LAUNCH_CHECK();
     }
     std::vector<emg_solve_info> inf(kb);
     solve_block_pow2(c, kb, f.data(), w.blk_rhs.p, w.blk_x.p, o, inf.data());
-    EMG_CUDA(cudaMemcpy2DAsync(x_dev + (size_t)j0 * 2, src_pitch, w.blk_x.p, dst_pitch, width, n,
-                               cudaMemcpyDeviceToDevice, c.stream));
+    scatter_cols_kernel<<<gs, 256, 0, c.stream>>>(n, k, kb, cm, (const double2 *)w.blk_x.p, (double2 *)x_dev);
+    EMG_LAUNCH_CHECK();
     total_s += c.kernel_ms["solve_block"] * 1e-3;
-    if (infos)
-      for (int j = 0; j < kc; ++j) infos[j0 + j] = inf[j];
-    for (int j = 0; j < kc && j < (int)c.block_initial_res.size(); ++j) r0[j0 + j] = c.block_initial_res[j];
+    for (int j = 0; j < cm.m; ++j) {
+      if (infos) infos[cm.src[j]] = inf[j];
+      if (j < (int)c.block_initial_res.size()) r0[cm.src[j]] = c.block_initial_res[j];
+    }
   }
+}
+
+// Any number of columns.  With the FP32 preconditioner, columns below
+// -emg_block_fp64_below Hz are solved as their own block with the FP64 one:
+// there the FP32 rounding noise left in the gradient space of the air reaches
+// the receiver fields at the 1e-3 level whatever the residual.
+static void solve_block_dev(Context &c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                            const emg_block_opts &o, emg_solve_info *infos) {
+  need(k >= 1, EMG_ERR_ARG, "block width k must be positive");
+  const bool fp32 = o.inner_fp32 < 0 ? c.opt.inner_fp32 != 0 : o.inner_fp32 != 0;
+  std::vector<int> lo, hi;
+  for (int j = 0; j < k; ++j) (fp32 && freqs[j] < c.opt.block_fp64_below_hz ? lo : hi).push_back(j);
+  double total_s = 0;
+  std::vector<double> r0(k, 1.0);
+  if (!lo.empty()) {
+    emg_block_opts o64 = o;
+    o64.inner_fp32 = 0;
+    solve_block_subset(c, lo, k, freqs, rhs_dev, x_dev, o64, infos, total_s, r0);
+  }
+  if (!hi.empty()) solve_block_subset(c, hi, k, freqs, rhs_dev, x_dev, o, infos, total_s, r0);
   EMG_CUDA(cudaStreamSynchronize(c.stream));
   c.kernel_ms["solve_block"] = total_s * 1e3;
   c.block_initial_res = r0;

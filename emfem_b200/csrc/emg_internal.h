@@ -171,6 +171,12 @@ struct Options {
   int smoother_cheb = 1;  // degree-2 Chebyshev (1) or l1-Jacobi (0) in AMS and AMG
   int gpu_amg = 1;        // nodal AMG setup on the device (1) or on the host (0)
   int block_fp64_fallback = 1;  // batched path: columns the FP32 AMS leaves unconverged finish in FP64
+  // batched path accuracy policy: the FP32 AMS leaves rounding noise in the
+  // near-null gradient space of the air, which the residual does not see but
+  // the receiver fields do; FP32-preconditioned columns iterate to rtol times
+  // this factor, and columns below block_fp64_below_hz use the FP64 AMS
+  double block_fp32_rtol_factor = 0.01;
+  double block_fp64_below_hz = 2e-3;
   // emg_*
   int inner_fp32 = 0;
   int graphs = 1;
