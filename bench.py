@@ -801,7 +801,7 @@ def ours(args):
             "converged": all_conv, "true_rel_res_max": max(c[0] for c in conv) if conv else None,
             "outer_its": [c[1] for c in conv],
             "roofline": roof, "profile_bins": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in bins.items()},
-            "phases_one_step": phases,
+            "phases_one_step": phases, "spmm_layouts": E.spmm_layouts(),
             "host_breakdown_s_per_step": timed_breakdown,
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "wall_s": wall,
         }

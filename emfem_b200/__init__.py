@@ -8,10 +8,10 @@ library or without a GPU every compute call raises.
 """
 
 from .api import (EMContext, EMGError, SolveInfo, lib, library_path, refine_fixed_fraction,
-                  refine_fixed_number, launch_count, profile_enable, profile_get, XY_POLAR, YX_POLAR,
+                  refine_fixed_number, launch_count, profile_enable, profile_get, spmm_layouts, XY_POLAR, YX_POLAR,
                   SOL_CSEM, SOL_DUAL, calculate_response_mt, calculate_response_csem, PointIndex, Survey)
 from . import meshgen
 
 __all__ = ["EMContext", "EMGError", "SolveInfo", "lib", "library_path", "refine_fixed_fraction",
-           "refine_fixed_number", "launch_count", "profile_enable", "profile_get", "XY_POLAR", "YX_POLAR", "SOL_CSEM", "SOL_DUAL", "calculate_response_mt",
+           "refine_fixed_number", "launch_count", "profile_enable", "profile_get", "spmm_layouts", "XY_POLAR", "YX_POLAR", "SOL_CSEM", "SOL_DUAL", "calculate_response_mt",
            "calculate_response_csem", "PointIndex", "Survey", "meshgen"]

@@ -98,6 +98,8 @@ _SIGS = {
     "emg_launch_count": ([C.POINTER(C.c_long)], _I),
     "emg_profile_enable": ([_I], _I),
     "emg_profile_get": ([C.c_char_p, C.POINTER(C.c_long), C.POINTER(_D), C.POINTER(_D)], _I),
+    "emg_spmm_layouts": ([C.c_char_p, C.c_long], _I),
+    "emg_divergence_correct_dev": ([_P, _I, _P, _P, _P, _I, C.POINTER(C.c_long)], _I),
     "emg_assemble_rhs_mt_block": ([_P, _I, _P, _P, _P], _I),
     "emg_assemble_rhs_mt_block_dev": ([_P, _I, _P, _P, _P], _I),
     "emg_estimate_error_noalloc": ([_P, _I, _I, _P, _P], _I),
@@ -165,6 +167,13 @@ def launch_count() -> int:
     n = C.c_long()
     _check(lib().emg_launch_count(C.byref(n)))
     return n.value
+
+
+def spmm_layouts() -> str:
+    """The SpMM lane layouts the autotuner chose so far (text)."""
+    buf = C.create_string_buffer(4096)
+    _check(lib().emg_spmm_layouts(buf, 4096))
+    return buf.value.decode()
 
 
 def profile_enable(on=True):
@@ -510,6 +519,14 @@ class EMContext:
         _check(lib().emg_solve_block_dev(self._h, k, _ptr(freqs), C.c_void_p(rhs_ptr), C.c_void_p(x_ptr),
                                          C.byref(o), C.cast(infos, C.c_void_p)))
         return list(infos)
+
+    def divergence_correct_dev(self, freqs, rhs_ptr, x_ptr, fp32=True):
+        """x += G phi (see emg_divergence_correct_dev); returns the FCG iterations."""
+        freqs = _f64(freqs)
+        its = C.c_long()
+        _check(lib().emg_divergence_correct_dev(self._h, freqs.size, _ptr(freqs), C.c_void_p(rhs_ptr),
+                                                C.c_void_p(x_ptr), int(bool(fp32)), C.byref(its)))
+        return its.value
 
     def interpolate_fields_block_dev(self, freqs, x_ptr, pts, tets):
         """E and H of every column of a device block (n_edges x k complex) at

@@ -119,6 +119,12 @@ struct Workspace {
   bool block_ready64 = false, block_ready32 = false;
   Ams<double> bams64;
   Ams<float> bams32;
+  // divergence correction of the batched path
+  Fcg<double> fcg_div;
+  DBuf<double> div_d, div_dis, div_ds;          // nv: l1 scale, its -1/2 and 1/2 powers (0 on the boundary)
+  DBuf<double> div_rhs, div_y, div_t, div_u;    // nv x K2
+  DBuf<double> div_e, div_me;                   // ne x K2
+  DBuf<float> div_tf, div_uf;                   // nv x K2, the FP32 hierarchy's operands
 };
 
 Context::Context() : ws(new Workspace()) {}
@@ -226,6 +232,9 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_block_fp64_fallback") o.block_fp64_fallback = v.empty() ? 1 : getb(v);
     else if (key == "emg_block_fp32_rtol_factor") o.block_fp32_rtol_factor = getr(k, v);
     else if (key == "emg_block_fp64_below") o.block_fp64_below_hz = getr(k, v);
+    else if (key == "emg_div_correction") o.div_correction = v.empty() ? 1 : getb(v);
+    else if (key == "emg_div_rtol") o.div_rtol = getr(k, v);
+    else if (key == "emg_div_max_it") o.div_max_it = geti(k, v);
     else if (key == "emg_fused_wait_ms") o.fused_wait_ms = getr(k, v);
     else if (key == "emg_fused_test_withhold") o.fused_test_withhold = geti(k, v);
     else if (key == "emg_pi_coupled") o.pi_coupled = v.empty() ? 1 : getb(v);
@@ -239,8 +248,9 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key.rfind("A_", 0) == 0 || key.rfind("B_", 0) == 0) ignored.push_back(k);
     else fail(EMG_ERR_OPTION, "unknown option %s", k.c_str());
   }
-  if (o.gmres_restart < 1 || o.gmres_restart > 32) fail(EMG_ERR_OPTION, "A_ksp_gmres_restart must be in [1, 32]");
+  if (o.gmres_restart < 1 || o.gmres_restart > 128) fail(EMG_ERR_OPTION, "A_ksp_gmres_restart must be in [1, 128]");
   if (o.block_fcg_check_every < 1) fail(EMG_ERR_OPTION, "-emg_block_fcg_check_every must be >= 1");
+  if (o.div_max_it < 1 || !(o.div_rtol > 0)) fail(EMG_ERR_OPTION, "-emg_div_max_it must be >= 1, -emg_div_rtol > 0");
   if (!(o.block_fp32_rtol_factor > 0 && o.block_fp32_rtol_factor <= 1))
     fail(EMG_ERR_OPTION, "-emg_block_fp32_rtol_factor must be in (0, 1]");
   if (o.fcg_mmax < 1 || o.fcg_mmax > 30 || o.block_fcg_mmax < 1 || o.block_fcg_mmax > 30)
@@ -641,6 +651,9 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_block_fp64_fallback") *value = o.block_fp64_fallback;
   else if (k == "emg_block_fp32_rtol_factor") *value = o.block_fp32_rtol_factor;
   else if (k == "emg_block_fp64_below") *value = o.block_fp64_below_hz;
+  else if (k == "emg_div_correction") *value = o.div_correction;
+  else if (k == "emg_div_rtol") *value = o.div_rtol;
+  else if (k == "emg_div_max_it") *value = o.div_max_it;
   else if (k == "emg_fused_wait_ms") *value = o.fused_wait_ms;
   else if (k == "emg_fused_test_withhold") *value = o.fused_test_withhold;
   else if (k == "emg_pi_coupled") *value = o.pi_coupled;
@@ -1264,6 +1277,164 @@ __global__ static void conj_copy_kernel(long n, const double2 *a, double2 *b) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// divergence correction of a block solution
+//
+// The FP32 AMS leaves rounding noise in the near-null space of A = C + i w Ms:
+// gradients in the air, where C G = 0 and w sigma_air is tiny, so the
+// residual hardly sees it while the receiver E fields do.  The exact solution
+// satisfies G^T (b - A x) = 0 at every interior vertex (the weak divergence
+// condition, div(sigma E) = source).  With r = b - A x, the vertex potential
+// phi (zero at boundary vertices, so the Dirichlet edges keep their values and
+// C G phi = 0) solving
+//     i w (G^T Ms G) phi = G^T r
+// restores it: x <- x + G phi removes the divergence error without touching
+// the curl part.  G^T Ms G is solved by FCG in FP64 on the symmetrically
+// scaled system D^-1/2 N D^-1/2 (D: the l1 scale of each vertex row, so that
+// air and earth rows converge alike), preconditioned by the gradient space's
+// nodal V-cycle of the block's AMS.
+// ---------------------------------------------------------------------------
+__global__ void div_scale_edges_kernel(int ne, const int *__restrict__ rp, const int *__restrict__ ci,
+                                       const double *__restrict__ ms, const int *__restrict__ edges,
+                                       const unsigned char *__restrict__ ebdr, double *__restrict__ d,
+                                       double *__restrict__ bnd) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  double m = 0;
+  for (int k = rp[e]; k < rp[e + 1]; ++k)
+    if (ci[k] == e) {
+      m = fabs(ms[k]);
+      break;
+    }
+  const int v0 = edges[2 * (long)e], v1 = edges[2 * (long)e + 1];
+  atomicAdd(d + v0, m);
+  atomicAdd(d + v1, m);
+  if (ebdr[e]) {
+    bnd[v0] = 1.0;
+    bnd[v1] = 1.0;
+  }
+}
+
+__global__ void div_scale_vertices_kernel(int nv, const double *__restrict__ d, const double *__restrict__ bnd,
+                                          double *__restrict__ dis, double *__restrict__ ds) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const bool in = bnd[v] == 0.0 && d[v] > 0.0;
+  dis[v] = in ? 1.0 / sqrt(d[v]) : 0.0;
+  ds[v] = in ? sqrt(d[v]) : 0.0;
+}
+
+// out = dis * (G^T r) / (i w_j) for nv x k complex entries
+__global__ void div_rhs_kernel(long total, int k, const double *__restrict__ omega, const double *__restrict__ dis,
+                               const double2 *__restrict__ gtr, double2 *__restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const long v = i / k;
+  const int j = (int)(i - v * k);
+  const double f = dis[v] / omega[j];
+  const double2 a = gtr[i];
+  out[i] = make_double2(a.y * f, -a.x * f);
+}
+
+extern "C++" {
+template <typename TI, typename TO>
+__global__ void vrow_scale_kernel(long total, int K, const double *__restrict__ sv, const TI *__restrict__ in,
+                                  TO *__restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  out[i] = (TO)(sv[i / K] * (double)in[i]);
+}
+
+template <typename TI, typename TO>
+static void vrow_scale(long rows, int K, const double *sv, const TI *in, TO *out, cudaStream_t s) {
+  const long total = rows * K;
+  vrow_scale_kernel<TI, TO><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, K, sv, in, out);
+  EMG_LAUNCH_CHECK();
+}
+}  // extern "C++"
+
+// x (ne x k complex, device) <- x + G phi; b is the right-hand side the block
+// solved (conjugated form), omega the k column frequencies (device); returns
+// the inner FCG iterations
+static long div_correct(Context &c, int k, bool fp32, const double *b, double *x, const double *omega) {
+  Workspace &w = *c.ws;
+  cudaStream_t s = c.stream;
+  const int ne = c.ne, nv = c.nv, K2 = 2 * k;
+  const size_t NV = (size_t)nv * K2, NE = (size_t)ne * K2;
+  w.div_d.alloc(nv);
+  w.div_dis.alloc(nv);
+  w.div_ds.alloc(nv);
+  w.div_rhs.alloc(NV);
+  w.div_y.alloc(NV);
+  w.div_t.alloc(NV);
+  w.div_u.alloc(NV);
+  w.div_e.alloc(NE);
+  w.div_me.alloc(NE);
+  // vertex scale and boundary mask (div_rhs holds the mask for a moment)
+  w.div_d.zero(s);
+  EMG_CUDA(cudaMemsetAsync(w.div_rhs.p, 0, sizeof(double) * nv, s));
+  div_scale_edges_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(ne, c.rp.p, c.ci.p, c.Msv.p, c.edges.p,
+                                                                      c.ebdr.p, w.div_d.p, w.div_rhs.p);
+  EMG_LAUNCH_CHECK();
+  div_scale_vertices_kernel<<<(unsigned)((nv + 255) / 256), 256, 0, s>>>(nv, w.div_d.p, w.div_rhs.p, w.div_dis.p,
+                                                                         w.div_ds.p);
+  EMG_LAUNCH_CHECK();
+  // right-hand side: D^-1/2 G^T (b - A x) / (i w)
+  spmm_complex(ne, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega, x, b, w.div_e.p, true, false, s);
+  ams_restrict<double>(nv, K2, 0, c.vinc_rp.p, c.vinc.p, nullptr, w.div_e.p, w.div_t.p, s);
+  {
+    const long total = (long)nv * k;
+    div_rhs_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(total, k, omega, w.div_dis.p,
+                                                                   (const double2 *)w.div_t.p,
+                                                                   (double2 *)w.div_rhs.p);
+    EMG_LAUNCH_CHECK();
+  }
+  // scaled operator: D^-1/2 G^T Ms G D^-1/2
+  auto op = [&](const double *p_, double *s_) {
+    vrow_scale<double, double>(nv, K2, w.div_dis.p, p_, w.div_t.p, s);
+    w.div_e.zero(s);
+    ams_prolong_add<double>(ne, K2, 0, c.edges.p, nullptr, w.div_t.p, w.div_e.p, s);
+    SpmmArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = ne;
+    a.rp = c.rp.p;
+    a.ci = c.ci.p;
+    a.vc = c.Msv.p;
+    a.vm = nullptr;
+    a.omega = omega;
+    a.x = w.div_e.p;
+    a.y = w.div_me.p;
+    a.relax_w = 1.0;
+    a.mode = SPMM_AX;
+    spmm_nnz<double>(K2, a, c.nnz, s);
+    ams_restrict<double>(nv, K2, 0, c.vinc_rp.p, c.vinc.p, nullptr, w.div_me.p, w.div_u.p, s);
+    vrow_scale<double, double>(nv, K2, w.div_dis.p, w.div_u.p, s_, s);
+  };
+  // scaled preconditioner: D^1/2 V D^1/2 with V the gradient space's V-cycle
+  auto pc = [&](const double *r_, double *z_) {
+    if (fp32) {
+      w.div_tf.alloc(NV);
+      w.div_uf.alloc(NV);
+      vrow_scale<double, float>(nv, K2, w.div_ds.p, r_, w.div_tf.p, s);
+      w.bams32.grad_vcycle(w.div_tf.p, w.div_uf.p, s);
+      vrow_scale<float, double>(nv, K2, w.div_ds.p, w.div_uf.p, z_, s);
+    } else {
+      vrow_scale<double, double>(nv, K2, w.div_ds.p, r_, w.div_t.p, s);
+      w.bams64.grad_vcycle(w.div_t.p, w.div_u.p, s);
+      vrow_scale<double, double>(nv, K2, w.div_ds.p, w.div_u.p, z_, s);
+    }
+  };
+  w.fcg_div.mmax = 2;
+  w.fcg_div.check_every = c.opt.block_fcg_check_every;
+  w.fcg_div.verbose = c.opt.verbose > 1;
+  w.fcg_div.total_its = 0;
+  w.fcg_div.solve_with(nv, K2, pc, op, w.div_rhs.p, w.div_y.p, c.opt.div_rtol, c.opt.div_max_it, s);
+  // x += G D^-1/2 y
+  vrow_scale<double, double>(nv, K2, w.div_dis.p, w.div_y.p, w.div_t.p, s);
+  ams_prolong_add<double>(ne, K2, 0, c.edges.p, nullptr, w.div_t.p, x, s);
+  return w.fcg_div.total_its;
+}
+
 // batched fast path on device vectors, one block of k (a power of two <= 32)
 // columns
 static void solve_block_pow2(Context &c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
@@ -1385,6 +1556,32 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
   if (fp32) w.bams32.check_fused(c.stream);
   else w.bams64.check_fused(c.stream);
   long inner = w.fcg64.total_its;
+  c.kernel_ms["div_correction"] = 0;
+  c.kernel_ms["div_its"] = 0;
+  if (c.opt.div_correction) {
+    auto td = std::chrono::steady_clock::now();
+    const long dits = div_correct(c, k, fp32, w.vec_a.p, x_dev, w.gm.omega.p);
+    // the true residual of the corrected solution
+    std::vector<double> rn(k), bn(k);
+    spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, w.gm.omega.p, x_dev, w.vec_a.p, w.gm.r.p, true, false,
+                 c.stream);
+    w.gm.nrm.zero(c.stream);
+    cnorm2(n, k, w.gm.r.p, w.gm.nrm.p, c.stream);
+    w.gm.nrm.download(rn.data(), k, c.stream);
+    w.gm.nrm.zero(c.stream);
+    cnorm2(n, k, w.vec_a.p, w.gm.nrm.p, c.stream);
+    w.gm.nrm.download(bn.data(), k, c.stream);
+    EMG_CUDA(cudaStreamSynchronize(c.stream));
+    const double rtol_c = (o.rtol > 0 ? o.rtol : c.opt.e_rtol) * (fp32 ? c.opt.block_fp32_rtol_factor : 1.0);
+    for (int j = 0; j < k; ++j) {
+      st.true_res[j] = bn[j] > 0 ? std::sqrt(rn[j] / bn[j]) : 0.0;
+      st.converged[j] = st.true_res[j] <= rtol_c * 1.0000001 || bn[j] == 0 ? 1 : 0;
+    }
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - td).count();
+    st.seconds += ms * 1e-3;
+    c.kernel_ms["div_correction"] = ms;
+    c.kernel_ms["div_its"] = (double)dits;
+  }
   if (infos)
     for (int j = 0; j < k; ++j) fill_info(&infos[j], st, inner, j);
   c.kernel_ms["solve_block"] = st.seconds * 1e3;
@@ -1523,6 +1720,36 @@ int emg_solve_block_dev(emg_context *c, int k, const double *freqs, const double
   EMG_API_END
 }
 
+int emg_divergence_correct_dev(emg_context *c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                               int fp32, long *its) {
+  EMG_API_BEGIN
+  need(c && freqs && rhs_dev && x_dev, EMG_ERR_ARG, "null argument");
+  need(k >= 1 && (k & (k - 1)) == 0 && k <= 32, EMG_ERR_ARG, "block width k must be a power of two <= 32");
+  need(c->assembled, EMG_ERR_STATE, "divergence correction before assemble_matrix");
+  use_device(*c);
+  Workspace &w = *c->ws;
+  need(fp32 ? w.block_ready32 : w.block_ready64, EMG_ERR_STATE,
+       "divergence correction before a block solve of that precision");
+  std::vector<double> om(k), col(2 * k);
+  for (int j = 0; j < k; ++j) {
+    need(freqs[j] > 0, EMG_ERR_ARG, "frequencies must be positive");
+    om[j] = 2 * PI * freqs[j];
+    col[2 * j] = col[2 * j + 1] = om[j];
+  }
+  if (fp32) w.bams32.set_columns(col, c->stream);
+  else w.bams64.set_columns(col, c->stream);
+  const long n = c->ne;
+  w.vec_a.alloc((size_t)n * k * 2);
+  conj_copy_kernel<<<(unsigned)((n * k + 255) / 256), 256, 0, c->stream>>>(n * k, (const double2 *)rhs_dev,
+                                                                          (double2 *)w.vec_a.p);
+  EMG_LAUNCH_CHECK();
+  w.gm.omega.upload(om, c->stream);
+  const long dits = div_correct(*c, k, fp32 != 0, w.vec_a.p, x_dev, w.gm.omega.p);
+  EMG_CUDA(cudaStreamSynchronize(c->stream));
+  if (its) *its = dits;
+  EMG_API_END
+}
+
 int emg_solve_block(emg_context *c, int k, const double *freqs, const double *rhs, double *x,
                     const emg_block_opts *opts, emg_solve_info *infos) {
   EMG_API_BEGIN
@@ -1602,6 +1829,16 @@ int emg_profile_enable(int on) {
   p.reset();
   p.enabled = on == 1;
   p.phases = on == 2;
+  EMG_API_END
+}
+
+int emg_spmm_layouts(char *buf, long len) {
+  EMG_API_BEGIN
+  need(buf && len > 0, EMG_ERR_ARG, "null argument");
+  const std::string r = tuner().report();
+  const size_t m = std::min((size_t)len - 1, r.size());
+  std::memcpy(buf, r.data(), m);
+  buf[m] = '\0';
   EMG_API_END
 }
 

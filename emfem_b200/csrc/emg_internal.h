@@ -171,12 +171,17 @@ struct Options {
   int smoother_cheb = 1;  // degree-2 Chebyshev (1) or l1-Jacobi (0) in AMS and AMG
   int gpu_amg = 1;        // nodal AMG setup on the device (1) or on the host (0)
   int block_fp64_fallback = 1;  // batched path: columns the FP32 AMS leaves unconverged finish in FP64
-  // batched path accuracy policy: the FP32 AMS leaves rounding noise in the
-  // near-null gradient space of the air, which the residual does not see but
-  // the receiver fields do; FP32-preconditioned columns iterate to rtol times
-  // this factor, and columns below block_fp64_below_hz use the FP64 AMS
-  double block_fp32_rtol_factor = 0.01;
-  double block_fp64_below_hz = 2e-3;
+  // batched path accuracy policy: FP32-preconditioned columns iterate to rtol
+  // times this factor (their receiver H error at a given residual is up to
+  // 10x that of an FP64-preconditioned solve), and columns below
+  // block_fp64_below_hz are solved with the FP64 AMS (0: none)
+  double block_fp32_rtol_factor = 0.1;
+  double block_fp64_below_hz = 0;
+  // divergence correction after every block solve: x += G phi with phi the
+  // vertex potential that makes G^T (b - A x) vanish at interior vertices
+  int div_correction = 1;
+  double div_rtol = 1e-9;
+  int div_max_it = 100;
   // emg_*
   int inner_fp32 = 0;
   int graphs = 1;

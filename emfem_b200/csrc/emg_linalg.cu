@@ -104,8 +104,9 @@ SpmmTuner &tuner() {
 std::string SpmmTuner::report() const {
   std::ostringstream os;
   for (auto &kv : best)
-    os << "T" << std::get<0>(kv.first) * 8 << " K" << std::get<1>(kv.first) << " bucket" << std::get<2>(kv.first)
-       << ": V=" << kv.second.first << " NL=" << kv.second.second << "; ";
+    os << "T" << std::get<0>(kv.first) * 8 << " K" << std::get<1>(kv.first) << " nnz/row class "
+       << std::get<2>(kv.first) << " rows class " << std::get<3>(kv.first) << ": V=" << kv.second.first
+       << (kv.second.second < 0 ? " rows kernel B=" : " NL=") << std::abs(kv.second.second) << "; ";
   return os.str();
 }
 
@@ -113,6 +114,9 @@ static int row_bucket(const SpmmArgs &a, long nnz) {
   double avg = a.n > 0 ? (double)nnz / a.n : 0;
   return avg < 6 ? 0 : (avg < 12 ? 1 : (avg < 24 ? 2 : 3));
 }
+
+// row-count class: the edge matrix and the finest nodal levels tune apart
+static int size_class(const SpmmArgs &a) { return a.n >= 1000000 ? 2 : (a.n >= 100000 ? 1 : 0); }
 
 template <typename T>
 static std::pair<int, int> spmm_default(int K, double avg) {
@@ -131,7 +135,7 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
   if (a.n <= 0) return;
   SpmmTuner &tn = tuner();
   int bucket = row_bucket(a, nnz);
-  auto key = std::make_tuple((int)sizeof(T), K, bucket);
+  auto key = std::make_tuple((int)sizeof(T), K, bucket, size_class(a));
   auto it = tn.best.find(key);
   std::pair<int, int> cfg;
   if (it != tn.best.end()) {
@@ -720,13 +724,17 @@ void cmultidot(int n, int K, int J, const double *V, long stride, const double *
                int partial_blocks, cudaStream_t s) {
   (void)partial;
   (void)partial_blocks;
-  if (J > MAXJ) fail(EMG_ERR_ARG, "restart above %d", MAXJ);
   if (K > 32) fail(EMG_ERR_ARG, "complex block width above 32");
   EMG_CUDA(cudaMemsetAsync(h, 0, sizeof(double) * 2 * J * K, s));
   long total = (long)n * K;
   unsigned grid = (unsigned)std::max(1L, std::min((total + 255) / 256, 148L * 2));
-  cmultidot_kernel<<<grid, 256, 0, s>>>(total, K, J, (const double2 *)V, stride / 2, (const double2 *)w, h);
-  EMG_LAUNCH_CHECK();
+  // at most MAXJ basis vectors per pass (their partial sums live in registers)
+  for (int j0 = 0; j0 < J; j0 += MAXJ) {
+    const int jc = std::min(MAXJ, J - j0);
+    cmultidot_kernel<<<grid, 256, 0, s>>>(total, K, jc, (const double2 *)(V + (size_t)j0 * stride), stride / 2,
+                                          (const double2 *)w, h + 2L * j0 * K);
+    EMG_LAUNCH_CHECK();
+  }
 }
 
 __global__ void __launch_bounds__(256) cgs_update_kernel(long total, int K, int J, const double2 *__restrict__ V,

@@ -17,7 +17,8 @@ namespace emg {
 // class).  Tuning runs on the first large non-accumulating call it sees and
 // times every legal (V, NL) candidate with CUDA events.
 struct SpmmTuner {
-  std::map<std::tuple<int, int, int>, std::pair<int, int>> best;  // (sizeof T, K, bucket) -> (V, NL)
+  // (sizeof T, K, nonzeros-per-row class, row-count class) -> (V, NL)
+  std::map<std::tuple<int, int, int, int>, std::pair<int, int>> best;
   bool allow_tuning = true;
   int tuned_count = 0;
   std::string report() const;

@@ -804,6 +804,16 @@ void Ams<T>::apply(const T *b, T *x, cudaStream_t s) {
 }
 
 template <typename T>
+void Ams<T>::grad_vcycle(const T *b, T *x, cudaStream_t s) {
+  if (fused) prepare_fused(s);
+  ensure_workspace(s);
+  const size_t bytes = sizeof(T) * (size_t)nv * K;
+  EMG_CUDA(cudaMemcpyAsync(wb[0][0].p, b, bytes, cudaMemcpyDeviceToDevice, s));
+  run_vcycle(0, s);
+  EMG_CUDA(cudaMemcpyAsync(x, wx[0][0].p, bytes, cudaMemcpyDeviceToDevice, s));
+}
+
+template <typename T>
 void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
   // count out-of-place edge smoothing applications to choose the start buffer
   int zeros = 0;
@@ -1217,7 +1227,7 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   cudaStream_t s = c.stream;
   n = c.ne;
   const int J = restart;
-  if (J < 1 || J > 32) fail(EMG_ERR_ARG, "FGMRES restart must be in 1..32");
+  if (J < 1 || J > 128) fail(EMG_ERR_ARG, "FGMRES restart must be in 1..128");
   if (k > 1024) fail(EMG_ERR_ARG, "block FGMRES supports at most 1024 columns");
   const size_t N2 = (size_t)n * k * 2;  // doubles per block vector
   V.alloc(N2 * (J + 1));

@@ -152,6 +152,9 @@ struct Ams {
   void apply(const T *b, T *x, cudaStream_t s);
   void apply_eager(const T *b, T *x, cudaStream_t s);
   const T *gphi() const { return wx[0][0].p; }  // gradient potential (split form)
+  // one V-cycle of the gradient space's nodal hierarchy on K vertex columns
+  // (b, x: nv x K, device); the divergence correction's preconditioner
+  void grad_vcycle(const T *b, T *x, cudaStream_t s);
   void spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s);
   size_t device_bytes() const;
 

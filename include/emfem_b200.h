@@ -285,6 +285,17 @@ int emg_solve_block(emg_context *ctx, int k, const double *freqs, const double *
                     const emg_block_opts *opts, emg_solve_info *infos);
 int emg_solve_block_dev(emg_context *ctx, int k, const double *freqs, const double *rhs_dev, double *x_dev,
                         const emg_block_opts *opts, emg_solve_info *infos);
+/* Divergence correction of a block solution x (device, n x k complex, the
+ * right-hand sides rhs_dev as emg_solve_block_dev takes them): x += G phi with
+ * phi the vertex potential, zero on the Dirichlet boundary, that makes
+ * G^T (b - A x) vanish at every interior vertex (b = conj(rhs), A = C + i w Ms),
+ * solved by FCG with the block AMS's gradient-space V-cycle (fp32 selects
+ * the FP32 or the FP64 hierarchy; the block solves run it after every solve
+ * unless -emg_div_correction 0).  k: a power of two <= 32, after an
+ * emg_solve_block(_dev) that set up the hierarchy of that precision.
+ * its: total FCG iterations over the columns (may be NULL). */
+int emg_divergence_correct_dev(emg_context *ctx, int k, const double *freqs, const double *rhs_dev, double *x_dev,
+                               int fp32, long *its);
 
 /* interpolate_fields (src/em_fwd.cc:719-744) for a device block x_dev (n_edges
  * x k complex, interleaved, as emg_solve_block_dev returns it) at n receivers
@@ -381,6 +392,10 @@ int emg_launch_count(long *n);
  * bytes accumulated since emg_profile_enable(1) */
 int emg_profile_enable(int on);
 int emg_profile_get(const char *bin, long *count, double *ms, double *bytes);
+/* the SpMM lane layouts the autotuner chose so far, one entry per (precision,
+ * block width, nonzeros-per-row class, row-count class), as text into
+ * buf[0..len) (NUL-terminated, truncated to fit) */
+int emg_spmm_layouts(char *buf, long len);
 
 #ifdef __cplusplus
 }

@@ -46,7 +46,7 @@ def test_options_parsing():
         assert c.get_option("B_ksp_rtol") == 0.05
         assert c.get_option("emg_inner_precision") == 1
         assert c.get_option("save_mesh") == 0
-        for bad in ("-bogus 1", "-K_max_it abc", "-inner_pc_type lu", "-A_ksp_gmres_restart 99",
+        for bad in ("-bogus 1", "-K_max_it abc", "-inner_pc_type lu", "-A_ksp_gmres_restart 999",
                     "-B_pc_hypre_ams_cycle_type 2", "stray"):
             with pytest.raises(E.EMGError) as ei:
                 c.process_options(bad)

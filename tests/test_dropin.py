@@ -121,4 +121,6 @@ def test_dropin_device_sequence(problem, tmp_path):
     # the solve accuracy, not bit for bit
     assert np.abs(zd - z).max() <= 1e-6 * np.abs(z).max()
     assert np.abs(_read(tmp, "out_csem_error") - err[0]).max() <= 1e-6 * np.abs(err[0]).max()
-    assert np.abs(_read(tmp, "out_pc_s") - x).max() <= 1e-6 * np.abs(x).max()
+    # pc_apply_b is an FCG solve stopped at 1e-2: rounding differences of the
+    # two processes' reductions move its iterate by more than the outer solve's
+    assert np.abs(_read(tmp, "out_pc_s") - x).max() <= 1e-4 * np.abs(x).max()

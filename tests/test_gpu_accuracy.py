@@ -4,9 +4,10 @@
 The path is emg_solve_block exactly as bench.py runs it: FP64 outer FGMRES to
 a relative residual of 1e-8 (the metric's setting), inner FCG capped at 30
 iterations with truncation 2, FP32 AMS with cycle "0201", and the batched
-path's accuracy policy (FP32-preconditioned columns iterate to 1e-8 x 0.01,
-columns below 2e-3 Hz take the FP64 AMS).  Right-hand sides come from the
-device block kernels.
+path's accuracy policy (FP32-preconditioned columns iterate to 1e-8 x 0.1,
+then the divergence correction takes the FP32 rounding noise out of the
+gradient space of the air).  Right-hand sides come from the device block
+kernels.
 
 Three solutions of each column are compared with the exact discrete solution
 (a sparse direct FP64 factorisation; configuration 0) or with the FP64 path at
