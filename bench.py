@@ -282,14 +282,15 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
         loss = ctx.warm_start_train(fa, fsa, xa.data_ptr(), src_pos=pos_a, steps=args.warm_steps,
                                     batch=args.warm_batch, lr=2e-3, seed=11)
         ctx.warm_start_predict(fa, fsa, xa.data_ptr(), ft, fst, xt.data_ptr(), src_pos=pos_a, tsrc_pos=pos_t,
-                               network=True)
+                               network=2)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         inf_t = ctx.solve_block_dev(ft, st.data_ptr(), xt.data_ptr(), rtol=1e-8, max_it=200, inner_fp32=True,
                                     use_guess=True)
         torch.cuda.synchronize()
         t3 = time.perf_counter()
-        rec.update(loss=loss, inf_a=inf_a, inf_t=inf_t, r0=ctx.last_initial_residuals(kt), t_anchor=t1 - t0,
+        rec.update(loss=loss, losses=ctx.warm_start_losses(), inf_a=inf_a, inf_t=inf_t,
+                   r0=ctx.last_initial_residuals(kt), t_anchor=t1 - t0,
                    t_net=t2 - t1, t_target=t3 - t2)
         return t3 - t0
 
@@ -318,16 +319,21 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
     out = {
         "network": ("per-edge MLP, 13 inputs (2 neighbour-frequency values scaled per edge, log resistivities, "
                     "log length, direction cosines, log distance to the source, log f, tau), 3 hidden layers of 64 "
-                    "with GELU, correction to the log-f interpolation; BF16 weights, FP32 accumulation, tcgen05 "
+                    "with GELU, output the curvature in log f (q = (lg f - lg f_a)(lg f - lg f_b) times it corrects the log-f "
+                    "interpolation); BF16 weights, FP32 accumulation, tcgen05 "
                     "forward and backward kernels, Adam"),
         "schedule": ("anchor columns (frequencies %s, every source) solved from zero; network trained on them "
-                     "(%d Adam steps of %d samples); the other %d columns solved from its guess"
+                     "(%d Adam steps of %d samples); the other %d columns solved from its guess (the network's "
+                     "correction only where its training loss is a quarter of the interpolation's)"
                      % ([float(f) for f in cols.freqs[::2]], args.warm_steps, args.warm_batch, kt)),
         "value": cols.k / t_step, "unit": UNIT, "ms_per_step": 1e3 * t_step, "steps_timed": n_t,
         "timing": "host wall clock around the whole two-stage step (assembly, right-hand sides, both solves, "
                   "training and prediction), after %d untimed steps" % max(1, min(args.warmup, 2)),
         "anchor_block_ms": 1e3 * rec["t_anchor"], "network_ms": 1e3 * rec["t_net"],
         "target_block_ms": 1e3 * rec["t_target"], "train_loss": rec["loss"],
+        "train_loss_interpolation": rec["losses"][1],
+        "guess": ("network" if 0 <= rec["losses"][0] <= 0.25 * rec["losses"][1] else
+                  "interpolation (the network's training loss was above a quarter of the interpolation's)"),
         "anchor_outer_its": [i.outer_its for i in rec["inf_a"]],
         "anchor_inner_its": int(rec["inf_a"][0].inner_its),
         "target_outer_its_network": [i.outer_its for i in rec["inf_t"]],

@@ -119,6 +119,7 @@ _SIGS = {
     "emg_warm_start_params": ([_P, _P, _P, C.POINTER(_I)], _I),
     "emg_warm_start_gradients": ([_P, _I, _P, _P, _P, _P, C.c_long, _I, _P, C.POINTER(_D)], _I),
     "emg_warm_start_reset": ([_P], _I),
+    "emg_warm_start_losses": ([_P, C.POINTER(_D), C.POINTER(_D)], _I),
     "emg_assemble_rhs_csem_block_dev": ([_P, _I, _P, _P, _P], _I),
     "emg_assemble_rhs_dual_block_dev": ([_P, _I, _I, _P, _P], _I),
     "emg_survey_read_emd": ([C.c_char_p], _P),
@@ -587,7 +588,8 @@ class EMContext:
         tf, ts, tp = self._cols(tfreqs, tsrc, tsrc_pos)
         _check(lib().emg_warm_start_predict(self._h, f.size, _ptr(f), _ptr(s), None if p is None else _ptr(p),
                                             C.c_void_p(x_ptr), tf.size, _ptr(tf), _ptr(ts),
-                                            None if tp is None else _ptr(tp), int(bool(network)),
+                                            None if tp is None else _ptr(tp),
+                                            network if network in (0, 1, 2) else int(bool(network)),
                                             C.c_void_p(guess_ptr)))
 
     def warm_start_params(self, set_to=None):
@@ -610,6 +612,12 @@ class EMContext:
 
     def warm_start_reset(self):
         _check(lib().emg_warm_start_reset(self._h))
+
+    def warm_start_losses(self):
+        """(network loss, interpolation loss) of the last training step; -1 before training."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().emg_warm_start_losses(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def spmv_complex_dev(self, omegas, x_ptr, y_ptr, conj_out=False):
         om = _f64(omegas)

@@ -197,6 +197,7 @@ struct Options {
   int block_inner_max_it = 30;
   int block_fcg_mmax = 2;
   int block_fcg_check_every = 5;  // inner iterations between host looks at the column status
+  int block_relax_times = 2;      // edge smoothing sweeps per '0' of the batched path's AMS cycle
   int spmm_tiled = 0;         // edge-column SpMMs gather through per-tile shared memory
   int tiled_smem_kb = 64;     // shared memory budget of one tile
   int verbose = 0;

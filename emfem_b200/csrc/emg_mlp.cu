@@ -9,10 +9,11 @@
 // divided by s_e = max(|e_a|, |e_b|) (4), log10 of the horizontal and vertical
 // resistivity around the edge (2), log10 edge length (1), direction cosines
 // (3), log10 distance to the source (1), log10 f (1) and tau, the position of
-// f between the two neighbour frequencies in log f (1).  Output: a correction
-// added to the log-f interpolation e_a + tau (e_b - e_a) (in units of s_e);
-// zero-initialised last layer, so the untrained network is that
-// interpolation.
+// f between the two neighbour frequencies in log f (1).  Output: the
+// curvature in log f; q times it (q = (log10 f - log10 f_a)(log10 f -
+// log10 f_b)) is the correction added to the log-f interpolation
+// e_a + tau (e_b - e_a) (in units of s_e); zero-initialised last layer, so the
+// untrained network is that interpolation.
 //
 // One persistent CTA per SM runs 128-sample tiles through the whole network on
 // the 5th-generation tensor cores: BF16 operands in shared memory (no-swizzle
@@ -183,7 +184,8 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
   return x;
 }
 
-constexpr float kTargetClamp = 2.0f;
+constexpr float kTargetClamp = 4.0f;
+constexpr float kMinQ = 1e-4f;  // |q| below this: the target column is a neighbour, nothing to learn
 
 struct KArgs {
   const unsigned char *img;  // packed BF16 weight image (IMG_BYTES)
@@ -201,16 +203,17 @@ struct KArgs {
   float inv_batch;
   float *grad;        // training: 208 x 128 + 128 x 128 floats, the two products summed over CTAs
   double *loss;       // training: summed 0.5 |out - target|^2 / batch
+  double *loss0;      // training: summed 0.5 |target|^2 / batch (a zero correction: the interpolation)
   int *err;
 };
 
 // features, base and scale of one sample (zeros for an invalid one)
 __device__ __forceinline__ void sample_features(const KArgs &a, long s, bool valid, float (&f)[16], float &b0,
-                                                float &b1, double &scale, float &t0, float &t1, int &e,
+                                                float &b1, float &q, double &scale, float &t0, float &t1, int &e,
                                                 int &tcol) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) f[i] = 0.f;
-  b0 = b1 = t0 = t1 = 0.f;
+  b0 = b1 = t0 = t1 = q = 0.f;
   scale = 0.0;
   e = 0;
   tcol = 0;
@@ -254,13 +257,15 @@ __device__ __forceinline__ void sample_features(const KArgs &a, long s, bool val
   f[12] = p.tau;
   b0 = (1.f - p.tau) * f[0] + p.tau * f[2];
   b1 = (1.f - p.tau) * f[1] + p.tau * f[3];
-  if (a.mode == 2) {
-    // corrections larger than a few neighbour magnitudes are outliers
-    // (edges where both neighbours nearly vanish): clamped, so that a few of
-    // them do not dominate the squared loss
+  q = p.q;
+  if (a.mode == 2 && fabsf(q) >= kMinQ) {
+    // the target is the curvature (correction / q); values beyond a few
+    // neighbour magnitudes are outliers (edges where both neighbours nearly
+    // vanish): clamped, so that a few of them do not dominate the squared loss
     const double2 et = a.xs[(long)e * a.ks + p.tcol];
-    t0 = fminf(fmaxf((float)(et.x * inv) - b0, -kTargetClamp), kTargetClamp);
-    t1 = fminf(fmaxf((float)(et.y * inv) - b1, -kTargetClamp), kTargetClamp);
+    const float iq = 1.f / q;
+    t0 = fminf(fmaxf(((float)(et.x * inv) - b0) * iq, -kTargetClamp), kTargetClamp);
+    t1 = fminf(fmaxf(((float)(et.y * inv) - b1) * iq, -kTargetClamp), kTargetClamp);
   }
 }
 
@@ -309,7 +314,7 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(KArgs a) {
   uint32_t phase = 0;
   bool ok = true;
   bool first = true;
-  float loss_acc = 0.f;
+  float loss_acc = 0.f, loss0_acc = 0.f;
 
   // one MMA group: operands written by every thread are made visible to the
   // tensor core, thread 0 issues, everyone waits for the commit
@@ -340,10 +345,10 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(KArgs a) {
   for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
     const long s = tile * T + tid;
     const bool valid = s < a.nsamples;
-    float f[16], b0, b1, t0, t1;
+    float f[16], b0, b1, q, t0, t1;
     double scale;
     int e, tcol;
-    sample_features(a, s, valid, f, b0, b1, scale, t0, t1, e, tcol);
+    sample_features(a, s, valid, f, b0, b1, q, scale, t0, t1, e, tcol);
     float o0 = 0.f, o1 = 0.f;
     if (NET) {
       st_row8(sm + OFF_IN, tid, 0, 16, f);
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(KArgs a) {
     }
     if (!TRAIN) {
       if (valid) {
-        const double p0 = (double)(b0 + o0) * scale, p1 = (double)(b1 + o1) * scale;
+        const double p0 = (double)(b0 + q * o0) * scale, p1 = (double)(b1 + q * o1) * scale;
         a.out[(long)e * a.kt + tcol] = make_double2(p0, p1);
       }
       continue;
@@ -398,6 +403,7 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(KArgs a) {
     // ---- training: loss and backward ----
     const float d0 = valid ? (o0 - t0) : 0.f, d1 = valid ? (o1 - t1) : 0.f;
     loss_acc += 0.5f * (d0 * d0 + d1 * d1) * a.inv_batch;
+    loss0_acc += 0.5f * (t0 * t0 + t1 * t1) * a.inv_batch;
     {
       float g[16];
 #pragma unroll
@@ -464,10 +470,16 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(KArgs a) {
     }
   }
   if (TRAIN) {
-    float l = loss_acc;
+    float l = loss_acc, l0 = loss0_acc;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
-    if ((tid & 31) == 0) atomicAdd(a.loss, (double)l);
+    for (int off = 16; off > 0; off >>= 1) {
+      l += __shfl_xor_sync(0xffffffffu, l, off);
+      l0 += __shfl_xor_sync(0xffffffffu, l0, off);
+    }
+    if ((tid & 31) == 0) {
+      atomicAdd(a.loss, (double)l);
+      atomicAdd(a.loss0, (double)l0);
+    }
   }
   if (!ok && tid == 0) atomicExch(a.err, 1);
   // a wait that gave up: wait once more (bounded) for the tensor-core work
@@ -633,6 +645,7 @@ void WarmStartNet::init(uint64_t seed, cudaStream_t s) {
   bias.zero(s);
   grad.alloc(128 * 208 + 128 * 128);
   loss.alloc(1);
+  loss0.alloc(1);
   err.alloc(1);
   err.zero(s);
   pack_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(params.p, img.p, bias.p);
@@ -708,6 +721,7 @@ double WarmStartNet::train_step(Context &c, const double *xs, int ks, const std:
   specs_dev.upload(specs, s);
   grad.zero(s);
   loss.zero(s);
+  loss0.zero(s);
   KArgs a;
   std::memset(&a, 0, sizeof(a));
   a.img = img.p;
@@ -724,6 +738,7 @@ double WarmStartNet::train_step(Context &c, const double *xs, int ks, const std:
   a.inv_batch = 1.0f / (float)batch;
   a.grad = grad.p;
   a.loss = loss.p;
+  a.loss0 = loss0.p;
   a.err = err.p;
   const long tiles = (batch + T - 1) / T;
   launch_mlp(2, a, (int)std::min<long>(tiles, sm_count(c.device)), s);

@@ -14,11 +14,16 @@ namespace emg {
 // source, tau = log(f / f_a) / log(f_b / f_a), logf = log10(f) / 2; tcol is
 // the column written (prediction) or the solved column learned (training).
 // src_kind 0: plane wave (distance = depth), 1: point source at src.
+// q = (log10 f - log10 f_a)(log10 f - log10 f_b): the error of the linear
+// interpolation in log f is half the second derivative times q, so the
+// network learns that curvature and the correction it adds is q times its
+// output -- which carries over between neighbour spacings (training pairs
+// are twice as far apart as the prediction pairs of a sweep).
 struct Spec {
   int a, b, tcol, src_kind;
   float tau, logf;
   float src[3];
-  float pad;
+  float q;
 };
 
 struct WarmStartNet {
@@ -28,7 +33,10 @@ struct WarmStartNet {
   DBuf<unsigned char> img;       // BF16 weight operands in the tensor-core layout
   DBuf<float> bias;              // 4 x 64
   DBuf<float> grad;              // the two accumulated gradient products
-  DBuf<double> loss;
+  DBuf<double> loss, loss0;
+  // losses of the last training step: the network's, and that of a zero
+  // correction (the interpolation) on the same samples; -1 before training
+  double last_loss = -1, last_loss0 = -1;
   DBuf<int> err;
   DBuf<float4> stat;             // 3 per edge
   int stat_ne = 0;

@@ -189,7 +189,9 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   ams.inc_rp = c.vinc_rp.p;
   ams.inc = c.vinc.p;
   ams.cycle = c.opt.ams_cycle;
-  ams.relax_times = c.opt.ams_relax_times;
+  // the batched path's own sweep count: with its capped inner solves, two
+  // edge sweeps per smoothing step cut the AMS applications by a quarter
+  ams.relax_times = per_frequency ? c.opt.ams_relax_times : c.opt.block_relax_times;
   ams.relax_w = c.opt.ams_relax_weight;
   ams.amg_relax_times = c.opt.amg_relax_times;
   ams.cheb = c.opt.smoother_cheb;
@@ -1222,6 +1224,27 @@ __global__ void gm_lsq_kernel(int K, int J, int m, int real_form, GmDev st, doub
   }
 }
 
+// Dirichlet rows of A are diagonal (their off-diagonal C and all of Ms are
+// zeroed at assembly), so the exact solution's boundary values are
+// b_e / C_ee: a guess takes them from the right-hand side
+__global__ void guess_boundary_kernel(int ne, int k, const int *__restrict__ rp, const int *__restrict__ ci,
+                                      const double *__restrict__ cv, const unsigned char *__restrict__ ebdr,
+                                      const double2 *__restrict__ b, double2 *__restrict__ x) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne || !ebdr[e]) return;
+  double d = 0;
+  for (int q = rp[e]; q < rp[e + 1]; ++q)
+    if (ci[q] == e) {
+      d = cv[q];
+      break;
+    }
+  if (d == 0) return;
+  for (int j = 0; j < k; ++j) {
+    const double2 v = b[(long)e * k + j];
+    x[(long)e * k + j] = make_double2(v.x / d, v.y / d);
+  }
+}
+
 int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double rtol, int maxit, bool real_form,
                   const std::function<void(const double *, double *)> &precond, SolveStats &st) {
   cudaStream_t s = c.stream;
@@ -1281,6 +1304,11 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   EMG_CUDA(cudaMemcpyAsync(gs.conv, conv0.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
   st.initial_res.assign(k, 1.0);
   if (use_guess) {
+    if (!real_form) {
+      guess_boundary_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, k, c.rp.p, c.ci.p, c.Cv.p, c.ebdr.p,
+                                                                        (const double2 *)b, (double2 *)x);
+      EMG_LAUNCH_CHECK();
+    }
     // the residual judges the guess: a column whose guess leaves a larger
     // residual than zero starts from zero instead
     spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, r.p, true, real_form, s);

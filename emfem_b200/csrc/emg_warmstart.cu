@@ -57,7 +57,7 @@ bool neighbours(const std::vector<Column> &solved, const Column &t, int skip, Sp
   sp.logf = (float)(0.5 * std::log10(t.f));
   sp.src_kind = t.point ? 1 : 0;
   for (int d = 0; d < 3; ++d) sp.src[d] = (float)t.pos[d];
-  sp.pad = 0.f;
+  sp.q = (float)((std::log10(t.f) - std::log10(fa)) * (std::log10(t.f) - std::log10(fb)));
   return true;
 }
 
@@ -107,9 +107,13 @@ int emg_warm_start_train(emg_context *c, int k, const double *freqs, const int *
     net.train_step(*c, x_dev, k, specs, o->batch, lr, false);
   }
   if (o->steps > 0) {
+    double l0 = 0.0;
     net.loss.download(&loss, 1, c->stream);
+    net.loss0.download(&l0, 1, c->stream);
     EMG_CUDA(cudaStreamSynchronize(c->stream));
     net.check(c->stream);
+    net.last_loss = loss;
+    net.last_loss0 = l0;
   }
   if (final_loss) *final_loss = loss;
   EMG_API_END
@@ -133,9 +137,23 @@ int emg_warm_start_predict(emg_context *c, int k, const double *freqs, const int
     sp.tcol = j;
     specs.push_back(sp);
   }
-  if (!specs.empty()) net.predict(*c, x_dev, k, specs, guess_dev, kt, network != 0);
+  need(network >= 0 && network <= 2, EMG_ERR_ARG, "network must be 0, 1 or 2");
+  // 2: the network only where training showed it halves the interpolation's
+  // curvature error (a quarter of its squared loss on the same samples)
+  const bool use_net = network == 1 || (network == 2 && net.last_loss >= 0 && net.last_loss0 > 0 &&
+                                        net.last_loss <= 0.25 * net.last_loss0);
+  if (!specs.empty()) net.predict(*c, x_dev, k, specs, guess_dev, kt, use_net);
   EMG_CUDA(cudaStreamSynchronize(c->stream));
   net.check(c->stream);
+  EMG_API_END
+}
+
+int emg_warm_start_losses(emg_context *c, double *loss, double *loss_interp) {
+  EMG_API_BEGIN
+  need(c && loss && loss_interp, EMG_ERR_ARG, "null argument");
+  WarmStartNet &net = net_of(*c);
+  *loss = net.last_loss;
+  *loss_interp = net.last_loss0;
   EMG_API_END
 }
 

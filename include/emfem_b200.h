@@ -352,8 +352,10 @@ typedef struct emg_warm_opts {
 int emg_warm_start_train(emg_context *ctx, int k, const double *freqs, const int *src, const double *src_pos,
                          const double *x_dev, const emg_warm_opts *opts, double *final_loss);
 /* guesses for kt target columns into guess_dev (n_edges x kt complex);
- * network 0: the log-f interpolation alone; a target without a solved
- * column of its source gets zero */
+ * network 0: the log-f interpolation alone, 1: interpolation plus the
+ * network's correction, 2: the network only if the last training step's loss
+ * was at most a quarter of the interpolation's on the same samples, else the
+ * interpolation; a target without a solved column of its source gets zero */
 int emg_warm_start_predict(emg_context *ctx, int k, const double *freqs, const int *src, const double *src_pos,
                            const double *x_dev, int kt, const double *tfreqs, const int *tsrc,
                            const double *tsrc_pos, int network, double *guess_dev);
@@ -366,6 +368,10 @@ int emg_warm_start_gradients(emg_context *ctx, int k, const double *freqs, const
                              const double *x_dev, long batch, int step, float *grads, double *loss);
 /* drops the network (the next use re-initialises it) */
 int emg_warm_start_reset(emg_context *ctx);
+/* losses of the last training step: the network's and that of the
+ * interpolation alone (a zero correction) on the same samples; -1 before
+ * any training */
+int emg_warm_start_losses(emg_context *ctx, double *loss, double *loss_interp);
 
 /* ---- kernel-level entry points on device pointers (tests, benchmarks) -- */
 /* y = (C + i w Ms) x  (conj_out=0)  or its conjugate (conj_out=1, the

@@ -86,7 +86,9 @@ def edge_statics(mesh, model):
 
 
 def training_specs(freqs, src, pos=None):
-    """(a, b, tcol, tau, logf, point, srcpos) per target, as the device builds them."""
+    """(a, b, tcol, tau, logf, q, point, srcpos) per target, as the device builds them;
+    q = (log10 f - log10 f_a)(log10 f - log10 f_b) scales the network's
+    output (a curvature in log f) into the correction."""
     specs = []
     for j in range(len(freqs)):
         cand = sorted((abs(math.log(freqs[i] / freqs[j])), i) for i in range(len(freqs))
@@ -97,13 +99,16 @@ def training_specs(freqs, src, pos=None):
         b = cand[1][1] if len(cand) > 1 else a
         fa, fb = freqs[a], freqs[b]
         tau = 0.0 if fa == fb else math.log(freqs[j] / fa) / math.log(fb / fa)
-        specs.append(dict(a=a, b=b, tcol=j, tau=np.float32(tau), logf=np.float32(0.5 * math.log10(freqs[j])),
+        lt = math.log10(freqs[j])
+        q = (lt - math.log10(fa)) * (lt - math.log10(fb))
+        specs.append(dict(a=a, b=b, tcol=j, tau=np.float32(tau), logf=np.float32(0.5 * lt), q=np.float32(q),
                           point=pos is not None, pos=None if pos is None else np.asarray(pos[j], np.float32)))
     return specs
 
 
 def features(stat, xs, spec, edges, with_target):
-    """Features (n x 16), base (n x 2), scale (n,), target correction (n x 2)."""
+    """Features (n x 16), base (n x 2), scale (n,), target curvature (n x 2):
+    the guess is (base + q * output) * scale."""
     ea, eb = xs[edges, spec["a"]], xs[edges, spec["b"]]
     sc = np.maximum(np.abs(ea), np.abs(eb))
     ok = sc > 1e-300
@@ -130,10 +135,12 @@ def features(stat, xs, spec, edges, with_target):
     base = np.stack([(np.float32(1) - tau) * f[:, 0] + tau * f[:, 2],
                      (np.float32(1) - tau) * f[:, 1] + tau * f[:, 3]], axis=1).astype(np.float32)
     tgt = np.zeros((n, 2), dtype=np.float32)
-    if with_target:
+    q = spec["q"]
+    if with_target and abs(q) >= np.float32(1e-4):
         et = xs[edges, spec["tcol"]]
-        tgt[:, 0] = np.clip((et.real * inv).astype(np.float32) - base[:, 0], -2.0, 2.0)
-        tgt[:, 1] = np.clip((et.imag * inv).astype(np.float32) - base[:, 1], -2.0, 2.0)
+        iq = np.float32(1) / q
+        tgt[:, 0] = np.clip(((et.real * inv).astype(np.float32) - base[:, 0]) * iq, -4.0, 4.0)
+        tgt[:, 1] = np.clip(((et.imag * inv).astype(np.float32) - base[:, 1]) * iq, -4.0, 4.0)
         tgt[~ok] = 0
     return f, base, np.where(ok, sc, 0.0), tgt
 
