@@ -77,6 +77,9 @@ def parse():
     ap.add_argument("--warm-steps", type=int, default=300, help="Adam steps of the warm-start network")
     ap.add_argument("--warm-batch", type=int, default=65536, help="samples per Adam step")
     ap.add_argument("--breakdown", action="store_true", help="print per-phase host timings to stderr")
+    ap.add_argument("--no-profile", action="store_true",
+                    help="skip the profiled step and the phase step after the timed region (no roofline)")
+    ap.add_argument("--no-phases", action="store_true", help="skip the phase step after the timed region")
     ap.add_argument("--options", default="", help="extra solver options (process_options text)")
     return ap.parse_args()
 
@@ -602,29 +605,31 @@ def ours(args):
     log("timed: %.1f ms/step" % ms_step)
     # kernel attribution: one more step with the event profiler on (it runs
     # the AMS launch by launch, so it stays out of the timed region)
-    E.profile_enable(True)
-    tp0 = time.perf_counter()
-    step()
-    torch.cuda.synchronize()
-    prof_step_s = time.perf_counter() - tp0
-    bins = {}
-    for b in ("spmm_edge_fp32", "spmm_edge_fp64", "spmm_nodal_fp32", "spmm_nodal_fp64", "vcycle_fused_fp32"):
-        n, t, by = E.profile_get(b)
-        bins[b] = (n, t, by)
-    E.profile_enable(False)
-    log("profiled step: %.1f s" % prof_step_s)
-    # solver phases with graphs and fused launches kept: events around the
-    # outer FGMRES, each inner FCG solve, each AMS application and each FP64
-    # operator apply
-    E.profile_enable(2)
-    step()
-    torch.cuda.synchronize()
-    phases = {}
-    for b in ("phase_fgmres", "phase_fcg", "phase_ams", "phase_opB"):
-        n, t, _ = E.profile_get(b)
-        phases[b[6:]] = {"count": n, "ms": round(t, 2)}
-    E.profile_enable(False)
-    log("phases: %s" % phases)
+    bins, phases, prof_step_s = {}, None, 0.0
+    if not args.no_profile:
+        E.profile_enable(True)
+        tp0 = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        prof_step_s = time.perf_counter() - tp0
+        for b in ("spmm_edge_fp32", "spmm_edge_fp64", "spmm_nodal_fp32", "spmm_nodal_fp64", "vcycle_fused_fp32"):
+            n, t, by = E.profile_get(b)
+            bins[b] = (n, t, by)
+        E.profile_enable(False)
+        log("profiled step: %.1f s" % prof_step_s)
+    if not args.no_profile and not args.no_phases:
+        # solver phases with graphs and fused launches kept: events around the
+        # outer FGMRES, each inner FCG solve, each AMS application and each FP64
+        # operator apply
+        E.profile_enable(2)
+        step()
+        torch.cuda.synchronize()
+        phases = {}
+        for b in ("phase_fgmres", "phase_fcg", "phase_ams", "phase_opB"):
+            n, t, _ = E.profile_get(b)
+            phases[b[6:]] = {"count": n, "ms": round(t, 2)}
+        E.profile_enable(False)
+        log("phases: %s" % phases)
     infos_headline = list(infos_last)
 
     # ---- learned warm start: anchors, training, predicted remainder ---------
@@ -661,7 +666,7 @@ def ours(args):
     # one kernel that streams HBM; the nodal-level SpMMs (many small, L2-resident launch
     # shapes, bound by dependent steps) are reported beside it as a share
     dom = "spmm_edge_fp32"
-    n_l, t_l, b_l = bins[dom]
+    n_l, t_l, b_l = bins.get(dom, (0, 0.0, 0.0))
     peak, peak_kind = peaks()
     achieved = (b_l / max(n_l, 1)) / ((t_l / max(n_l, 1)) * 1e-3) / 1e9 if n_l else 0.0
     traffic, traffic_ratio = roofline_traffic(dom, b_l / max(n_l, 1))
@@ -806,7 +811,7 @@ def ours(args):
             "speedup_vs_plain_fp64": (value / world) / plain["value"] if plain else None,
             "converged": all_conv, "true_rel_res_max": max(c[0] for c in conv) if conv else None,
             "outer_its": [c[1] for c in conv],
-            "roofline": roof, "profile_bins": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in bins.items()},
+            "roofline": roof if n_l else None, "profile_bins": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in bins.items()},
             "phases_one_step": phases, "spmm_layouts": E.spmm_layouts(),
             "host_breakdown_s_per_step": timed_breakdown,
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "wall_s": wall,
