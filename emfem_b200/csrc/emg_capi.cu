@@ -1502,6 +1502,7 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
   if (fp32) w.omega_cols.upload(col, c.stream);
   auto opB64 = [&](const double *p_, double *s_) {
     SpmmArgs a;
+    std::memset(&a, 0, sizeof(a));
     a.n = n;
     a.rp = c.rp.p;
     a.ci = c.ci.p;

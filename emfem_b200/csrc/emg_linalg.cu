@@ -21,7 +21,7 @@ constexpr bool spmm_legal() {
   return (K % V) == 0 && (K / V) * NL <= 32 && (32 % ((K / V) * NL)) == 0 && sizeof(T) * V <= 16;
 }
 
-template <typename T, int K, int V, int NL>
+template <typename T, int K, int V, int NL, bool PK = false>
 void spmm_launch(const SpmmArgs &a, cudaStream_t s) {
   constexpr int G = NL * (K / V);
   constexpr int RPW = 32 / G;
@@ -29,7 +29,7 @@ void spmm_launch(const SpmmArgs &a, cudaStream_t s) {
   long threads = warps * 32;
   unsigned grid = (unsigned)((threads + 255) / 256);
   if (grid == 0) return;
-  spmm_kernel<T, K, V, NL><<<grid, 256, 0, s>>>(a);
+  spmm_kernel<T, K, V, NL, PK><<<grid, 256, 0, s>>>(a);
 }
 
 // row-group kernel (spmm_rows_kernel): nl = -B selects it with B gathers in
@@ -54,6 +54,13 @@ SpmmFn spmm_rows_pick() {
   else return nullptr;
 }
 
+// packed-record variant (nl = 100 + NL): FP32 two-part operators only
+template <typename T, int K, int V, int NL>
+SpmmFn spmm_pick_packed() {
+  if constexpr (spmm_legal<T, K, V, NL>() && sizeof(T) == 4) return &spmm_launch<T, K, V, NL, true>;
+  else return nullptr;
+}
+
 template <typename T, int K, int V, int NL>
 SpmmFn spmm_pick() {
   if constexpr (spmm_legal<T, K, V, NL>()) return &spmm_launch<T, K, V, NL>;
@@ -64,6 +71,9 @@ SpmmFn spmm_pick_nl(int nl) {
   switch (nl) {
   case -4: return spmm_rows_pick<T, K, V, 4>();
   case -8: return spmm_rows_pick<T, K, V, 8>();
+  case 101: return spmm_pick_packed<T, K, V, 1>();
+  case 102: return spmm_pick_packed<T, K, V, 2>();
+  case 104: return spmm_pick_packed<T, K, V, 4>();
   case 1: return spmm_pick<T, K, V, 1>();
   case 2: return spmm_pick<T, K, V, 2>();
   case 4: return spmm_pick<T, K, V, 4>();
@@ -105,8 +115,10 @@ std::string SpmmTuner::report() const {
   std::ostringstream os;
   for (auto &kv : best)
     os << "T" << std::get<0>(kv.first) * 8 << " K" << std::get<1>(kv.first) << " nnz/row class "
-       << std::get<2>(kv.first) << " rows class " << std::get<3>(kv.first) << ": V=" << kv.second.first
-       << (kv.second.second < 0 ? " rows kernel B=" : " NL=") << std::abs(kv.second.second) << "; ";
+       << std::get<2>(kv.first) << " rows class " << (std::get<3>(kv.first) >> 1) << ": V=" << kv.second.first
+       << (std::get<3>(kv.first) & 1 ? " (packed records available)" : "")
+       << (kv.second.second < 0 ? " rows kernel B=" : (kv.second.second > 100 ? " packed NL=" : " NL="))
+       << (kv.second.second > 100 ? kv.second.second - 100 : std::abs(kv.second.second)) << "; ";
   return os.str();
 }
 
@@ -135,7 +147,8 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
   if (a.n <= 0) return;
   SpmmTuner &tn = tuner();
   int bucket = row_bucket(a, nnz);
-  auto key = std::make_tuple((int)sizeof(T), K, bucket, size_class(a));
+  const bool packed = a.pk != nullptr && sizeof(T) == 4 && a.vm != nullptr;
+  auto key = std::make_tuple((int)sizeof(T), K, bucket, 2 * size_class(a) + (packed ? 1 : 0));
   auto it = tn.best.find(key);
   std::pair<int, int> cfg;
   if (it != tn.best.end()) {
@@ -151,7 +164,8 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
       EMG_CUDA(cudaEventCreate(&e1));
       float bestms = 1e30f;
       for (int v : {1, 2, 4})
-        for (int nl : {1, 2, 4, 8, 16, 32, -4, -8}) {
+        for (int nl : {1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104}) {
+          if (nl > 100 && !packed) continue;
           SpmmFn f = spmm_fn<T>(K, v, nl);
           if (!f) continue;
           f(a, s);  // warm-up

@@ -80,6 +80,9 @@ struct SpmmArgs {
   int mode;
   void *r, *d;             // Chebyshev work vectors (n x K)
   double c1, c2;           // Chebyshev coefficients (inv_theta in c1 for CHEB1)
+  // FP32 two-part operators may also come as one 16-byte record per nonzero
+  // (column, vc bits, vm bits, 0): one load per nonzero instead of three
+  const int4 *pk;
 };
 
 // One step of a fused nodal V-cycle (vcycle_fused_kernel): the operations a
@@ -182,7 +185,7 @@ __device__ __forceinline__ void spmm_epilogue(const SpmmArgs &a, int row, int cb
   epi_store<T, K, V>(a, row, cb, acc, w, two, e);
 }
 
-template <typename T, int K, int V, int NL>
+template <typename T, int K, int V, int NL, bool PK = false>
 __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
   constexpr int CL = K / V;
   constexpr int G = NL * CL;
@@ -220,9 +223,16 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
       for (int u = 0; u < U; ++u) {
         const int k = k0 + u * NL;
         ok[u] = k < ke;
-        j[u] = ok[u] ? __ldg(a.ci + k) : 0;
-        c[u] = ok[u] ? __ldg(vc + k) : T(0);
-        m[u] = (ok[u] && two) ? __ldg(vm + k) : T(0);
+        if constexpr (PK) {
+          const int4 rec = ok[u] ? __ldg(a.pk + k) : make_int4(0, 0, 0, 0);
+          j[u] = rec.x;
+          c[u] = (T)__int_as_float(rec.y);
+          m[u] = (T)__int_as_float(rec.z);
+        } else {
+          j[u] = ok[u] ? __ldg(a.ci + k) : 0;
+          c[u] = ok[u] ? __ldg(vc + k) : T(0);
+          m[u] = (ok[u] && two) ? __ldg(vm + k) : T(0);
+        }
       }
       T xv[U][V];
 #pragma unroll

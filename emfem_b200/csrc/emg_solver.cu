@@ -178,6 +178,12 @@ struct StageClock {
   }
 };
 
+__global__ void pack_records_kernel(long nnz, const int *__restrict__ ci, const float *__restrict__ vc,
+                                    const float *__restrict__ vm, int4 *__restrict__ out) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k < nnz) out[k] = make_int4(ci[k], __float_as_int(vc[k]), __float_as_int(vm[k]), 0);
+}
+
 template <typename T>
 void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_ref) {
   cudaStream_t s = c.stream;
@@ -238,6 +244,16 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
     l1_rowsum_kernel<T><<<gr, 256, 0, s>>>(c.ne, c.rp.p, c.Msv.p, nullptr, 0.0, ams.B.l1m.p);
   }
   EMG_LAUNCH_CHECK();
+  // FP32 two-part B also as one 16-byte record per nonzero for the SpMM's
+  // packed variant (the autotuner decides whether it is used)
+  if (sizeof(T) == 4 && !per_frequency) {
+    ams.Bpk.alloc(c.nnz);
+    pack_records_kernel<<<g, 256, 0, s>>>(c.nnz, c.ci.p, (const float *)ams.B.vc.p, (const float *)ams.B.vm.p,
+                                          ams.Bpk.p);
+    EMG_LAUNCH_CHECK();
+  } else {
+    ams.Bpk.release();
+  }
   // edge tangents x(v1) - x(v0)
   {
     std::vector<T> tg((size_t)c.ne * 3);
@@ -469,6 +485,8 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
 template <typename T>
 void Ams<T>::spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s) {
   SpmmArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.pk = Bpk.p;
   a.n = ne;
   a.rp = brp;
   a.ci = bci;
@@ -605,6 +623,7 @@ T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b,
   auto run = [&](int mode, const T *x, const T *bb, T *y, T *r, T *d, double c1, double c2) {
     SpmmArgs a;
     std::memset(&a, 0, sizeof(a));
+    a.pk = edge ? Bpk.p : nullptr;
     a.n = n;
     a.rp = edge ? brp : A->rp.p;
     a.ci = edge ? bci : A->ci.p;
@@ -849,6 +868,7 @@ void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
       } else {
         ams_restrict<T>(nv, K, 0, inc_rp, inc, nullptr, b, gtmp.p, s);
         SpmmArgs a;
+        std::memset(&a, 0, sizeof(a));
         a.n = nv;
         a.rp = grp;
         a.ci = gci;

@@ -103,6 +103,7 @@ struct Ams {
   };
   Context *ctx = nullptr;          // owner of the fixed patterns (tiled copies)
   DCsr<T> B;                       // values only: pattern is the context's
+  DBuf<int4> Bpk;                  // FP32 two-part B as packed records (column, vc, vm, 0); empty otherwise
   const int *brp = nullptr, *bci = nullptr;
   long nnzB = 0;
   bool two = true;  // two value parts (batched) or combined (one frequency)
