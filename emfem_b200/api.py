@@ -25,6 +25,7 @@ EMG_ERR_NOMEM = -5
 EMG_DIVERGED_ITS = -6
 EMG_DIVERGED_NANORINF = -7
 EMG_ERR_OPTION = -8
+EMG_STOPPED_AT_FLOOR = 1         # block column at the FP64 rounding floor of its residual
 
 XY_POLAR, YX_POLAR = -1, -2      # src/em_defs.h:39
 SOL_CSEM, SOL_DUAL = 0, 1
@@ -93,6 +94,7 @@ _SIGS = {
     "emg_solve_block": ([_P, _I, _P, _P, _P, C.POINTER(BlockOpts), _P], _I),
     "emg_solve_block_dev": ([_P, _I, _P, _P, _P, C.POINTER(BlockOpts), _P], _I),
     "emg_spmv_complex_dev": ([_P, _I, _P, _P, _P, _I], _I),
+    "emg_spmm_layout_dev": ([_P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "emg_last_kernel_ms": ([_P, C.c_char_p, C.POINTER(_D)], _I),
     "emg_stream_synchronize": ([_P], _I),
     "emg_launch_count": ([C.POINTER(C.c_long)], _I),
@@ -113,6 +115,7 @@ _SIGS = {
     "emg_save_vtk": ([_P, C.c_char_p, _I, _P, _P], _I),
     "emg_interpolate_fields_block_dev": ([_P, _I, _P, _P, _I, _P, _P, _P], _I),
     "emg_last_initial_residuals": ([_P, _I, _P], _I),
+    "emg_last_residual_floors": ([_P, _I, _P], _I),
     "emg_amg_levels": ([_P, _I, _I, _D, _I, C.POINTER(_I), _P], _I),
     "emg_warm_start_train": ([_P, _I, _P, _P, _P, _P, C.POINTER(WarmOpts), C.POINTER(_D)], _I),
     "emg_warm_start_predict": ([_P, _I, _P, _P, _P, _P, _I, _P, _P, _P, _I, _P], _I),
@@ -564,6 +567,13 @@ class EMContext:
         _check(lib().emg_last_initial_residuals(self._h, int(k), _ptr(out)))
         return out
 
+    def last_residual_floors(self, k):
+        """per column of the last block solve: u || |b| + |A||x| || / ||b||, the
+        relative residual below which the FP64 residual is rounding noise"""
+        out = np.zeros(int(k))
+        _check(lib().emg_last_residual_floors(self._h, int(k), _ptr(out)))
+        return out
+
     # -- learned warm start ----------------------------------------------------------------
     @staticmethod
     def _cols(freqs, src, pos):
@@ -623,6 +633,18 @@ class EMContext:
         om = _f64(omegas)
         _check(lib().emg_spmv_complex_dev(self._h, om.size, _ptr(om), C.c_void_p(x_ptr), C.c_void_p(y_ptr),
                                           int(conj_out)))
+
+    def spmm_layout_dev(self, fp32, omegas, x_ptr, b_ptr, y_ptr, v, variant):
+        """y = b - (C + w_c Ms) x on len(omegas) real columns with the lane
+        layout (v, variant) forced; False when the layout is not built for
+        that block width."""
+        om = _f64(omegas)
+        rc = lib().emg_spmm_layout_dev(self._h, int(bool(fp32)), om.size, int(v), int(variant), _ptr(om),
+                                       C.c_void_p(x_ptr), C.c_void_p(b_ptr), C.c_void_p(y_ptr))
+        if rc == EMG_ERR_ARG:
+            return False
+        _check(rc)
+        return True
 
     def interpolate_fields_host(self, fidx, pts, tets, e_re, e_im):
         """interpolate_fields (src/em_fwd.cc:719-744) from a host solution;

@@ -248,6 +248,11 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_block_fcg_mmax") o.block_fcg_mmax = geti(k, v);
     else if (key == "emg_block_fcg_check_every") o.block_fcg_check_every = geti(k, v);
     else if (key == "emg_block_relax_times") o.block_relax_times = geti(k, v);
+    else if (key == "emg_cheb_degree") o.cheb_degree = geti(k, v);
+    else if (key == "emg_block_cheb_degree") o.block_cheb_degree = geti(k, v);
+    else if (key == "emg_amg_cheb_degree") o.amg_cheb_degree = geti(k, v);
+    else if (key == "emg_restrict_smooth") o.restrict_j0 = v.empty() ? 1 : getb(v);
+    else if (key == "emg_block_floor_stop") o.block_floor_stop = v.empty() ? 1 : getb(v);
     else if (key == "emg_spmm_tiled") o.spmm_tiled = v.empty() ? 1 : getb(v);
     else if (key == "emg_tiled_smem_kb") o.tiled_smem_kb = geti(k, v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
@@ -261,6 +266,10 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     fail(EMG_ERR_OPTION, "-emg_block_fp32_rtol_factor must be in (0, 1]");
   if (o.fcg_mmax < 1 || o.fcg_mmax > 30 || o.block_fcg_mmax < 1 || o.block_fcg_mmax > 30)
     fail(EMG_ERR_OPTION, "FCG truncation lengths must be in [1, 30]");
+  if (o.cheb_degree < 2 || o.cheb_degree > 6 || o.block_cheb_degree < 2 || o.block_cheb_degree > 6 ||
+      o.amg_cheb_degree < 2 || o.amg_cheb_degree > 6)
+    fail(EMG_ERR_OPTION, "Chebyshev degrees (-emg_cheb_degree, -emg_block_cheb_degree, -emg_amg_cheb_degree) must be "
+                         "in [2, 6]");
   if (o.ams_relax_times < 1 || o.amg_relax_times < 1 || o.block_relax_times < 1)
     fail(EMG_ERR_OPTION, "relax times must be >= 1");
   if (o.inner_max_it < 1 || o.block_inner_max_it < 1) fail(EMG_ERR_OPTION, "inner iteration caps must be >= 1");
@@ -669,6 +678,11 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_block_fcg_mmax") *value = o.block_fcg_mmax;
   else if (k == "emg_block_fcg_check_every") *value = o.block_fcg_check_every;
   else if (k == "emg_block_relax_times") *value = o.block_relax_times;
+  else if (k == "emg_cheb_degree") *value = o.cheb_degree;
+  else if (k == "emg_block_cheb_degree") *value = o.block_cheb_degree;
+  else if (k == "emg_amg_cheb_degree") *value = o.amg_cheb_degree;
+  else if (k == "emg_restrict_smooth") *value = o.restrict_j0;
+  else if (k == "emg_block_floor_stop") *value = o.block_floor_stop;
   else if (k == "emg_spmm_tiled") *value = o.spmm_tiled;
   else if (k == "emg_tiled_smem_kb") *value = o.tiled_smem_kb;
   else fail(EMG_ERR_OPTION, "unknown option %s", key);
@@ -939,7 +953,9 @@ static void fill_info(emg_solve_info *info, const SolveStats &st, long inner, in
   info->outer_its = col >= 0 && col < (int)st.col_its.size() ? st.col_its[col] : st.outer_its;
   info->inner_its = (int)inner;
   info->true_rel_res = col >= 0 && col < (int)st.true_res.size() ? st.true_res[col] : 0.0;
-  info->reason = (col >= 0 && col < (int)st.converged.size() && !st.converged[col]) ? EMG_DIVERGED_ITS : 0;
+  info->reason = 0;
+  if (col >= 0 && col < (int)st.converged.size() && !st.converged[col])
+    info->reason = col < (int)st.at_floor.size() && st.at_floor[col] ? EMG_STOPPED_AT_FLOOR : EMG_DIVERGED_ITS;
   info->seconds = st.seconds;
 }
 
@@ -1485,6 +1501,7 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
   // with the FP64 fallback behind it, an FP32 column that stops making
   // progress (less than 2x over a restart cycle) is handed over early
   w.gm.stall_factor = (fp32 && c.opt.block_fp64_fallback) ? 0.5 : 0.0;
+  w.gm.floor_stop = c.opt.block_floor_stop != 0;
   w.gm.omega.upload(om, c.stream);
   w.fcg64.mmax = w.fcg32.mmax = c.opt.block_fcg_mmax;
   w.fcg64.check_every = w.fcg32.check_every = c.opt.block_fcg_check_every;
@@ -1595,6 +1612,8 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
     for (int j = 0; j < k; ++j) {
       st.true_res[j] = bn[j] > 0 ? std::sqrt(rn[j] / bn[j]) : 0.0;
       st.converged[j] = st.true_res[j] <= rtol_c * 1.0000001 || bn[j] == 0 ? 1 : 0;
+      if (j < (int)st.at_floor.size())
+        st.at_floor[j] = !st.converged[j] && w.gm.floor_stop && st.true_res[j] <= 2.0 * st.floor_res[j] ? 1 : 0;
     }
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - td).count();
     st.seconds += ms * 1e-3;
@@ -1604,7 +1623,7 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
     // the sigma-weighted mass), so a column's residual norm can rise past
     // rtol; such columns continue from the corrected solution
     bool all_ok = true;
-    for (int j = 0; j < k; ++j) all_ok = all_ok && st.converged[j];
+    for (int j = 0; j < k; ++j) all_ok = all_ok && st.settled(j);
     if (!all_ok) {
       SolveStats st2;
       w.gm.solve(c, w.vec_a.p, x_dev, true, rtol_c, o.max_it > 0 ? o.max_it : c.opt.K_max_it, false, pc, st2);
@@ -1614,6 +1633,8 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
         st.col_its[j] += st2.col_its[j];
         st.true_res[j] = st2.true_res[j];
         st.converged[j] = st2.converged[j];
+        st.floor_res[j] = st2.floor_res[j];
+        st.at_floor[j] = st2.at_floor[j];
       }
       inner = w.fcg64.total_its;
     }
@@ -1622,12 +1643,13 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
     for (int j = 0; j < k; ++j) fill_info(&infos[j], st, inner, j);
   c.kernel_ms["solve_block"] = st.seconds * 1e3;
   c.block_initial_res = st.initial_res;
+  c.block_floor_res = st.floor_res;
   // a column the FP32 preconditioner could not carry to rtol within max_it
   // (stagnation at low frequency) is finished with the FP64 preconditioner,
   // starting from where it stopped; converged columns pass through at the
   // cost of one residual
   bool all_conv = true;
-  for (int j = 0; j < k; ++j) all_conv = all_conv && st.converged[j];
+  for (int j = 0; j < k; ++j) all_conv = all_conv && st.settled(j);
   if (fp32 && !all_conv && c.opt.block_fp64_fallback) {
     emg_block_opts o2 = o;
     o2.inner_fp32 = 0;
@@ -1636,6 +1658,7 @@ static void solve_block_pow2(Context &c, int k, const double *freqs, const doubl
     std::vector<double> r0 = st.initial_res;
     const double s1 = st.seconds;
     solve_block_pow2(c, k, freqs, rhs_dev, x_dev, o2, inf2.data());
+    // block_floor_res now holds the FP64 pass's floors
     if (infos)
       for (int j = 0; j < k; ++j) {
         infos[j].outer_its += inf2[j].outer_its;
@@ -1680,7 +1703,8 @@ __global__ void scatter_cols_kernel(long n, int k, int kb, ColMap cm, const doub
 // in the inner solves) at its last column's frequency.
 static void solve_block_subset(Context &c, const std::vector<int> &idx, int k, const double *freqs,
                                const double *rhs_dev, double *x_dev, const emg_block_opts &o,
-                               emg_solve_info *infos, double &total_s, std::vector<double> &r0) {
+                               emg_solve_info *infos, double &total_s, std::vector<double> &r0,
+                               std::vector<double> &fl) {
   constexpr int kMaxBlock = 32;
   const int m = (int)idx.size();
   int kp = 1;
@@ -1689,6 +1713,7 @@ static void solve_block_subset(Context &c, const std::vector<int> &idx, int k, c
     solve_block_pow2(c, k, freqs, rhs_dev, x_dev, o, infos);
     total_s += c.kernel_ms["solve_block"] * 1e-3;
     for (int j = 0; j < k && j < (int)c.block_initial_res.size(); ++j) r0[j] = c.block_initial_res[j];
+    for (int j = 0; j < k && j < (int)c.block_floor_res.size(); ++j) fl[j] = c.block_floor_res[j];
     return;
   }
   Workspace &w = *c.ws;
@@ -1720,6 +1745,7 @@ static void solve_block_subset(Context &c, const std::vector<int> &idx, int k, c
     for (int j = 0; j < cm.m; ++j) {
       if (infos) infos[cm.src[j]] = inf[j];
       if (j < (int)c.block_initial_res.size()) r0[cm.src[j]] = c.block_initial_res[j];
+      if (j < (int)c.block_floor_res.size()) fl[cm.src[j]] = c.block_floor_res[j];
     }
   }
 }
@@ -1735,16 +1761,17 @@ static void solve_block_dev(Context &c, int k, const double *freqs, const double
   std::vector<int> lo, hi;
   for (int j = 0; j < k; ++j) (fp32 && freqs[j] < c.opt.block_fp64_below_hz ? lo : hi).push_back(j);
   double total_s = 0;
-  std::vector<double> r0(k, 1.0);
+  std::vector<double> r0(k, 1.0), fl(k, 0.0);
   if (!lo.empty()) {
     emg_block_opts o64 = o;
     o64.inner_fp32 = 0;
-    solve_block_subset(c, lo, k, freqs, rhs_dev, x_dev, o64, infos, total_s, r0);
+    solve_block_subset(c, lo, k, freqs, rhs_dev, x_dev, o64, infos, total_s, r0, fl);
   }
-  if (!hi.empty()) solve_block_subset(c, hi, k, freqs, rhs_dev, x_dev, o, infos, total_s, r0);
+  if (!hi.empty()) solve_block_subset(c, hi, k, freqs, rhs_dev, x_dev, o, infos, total_s, r0, fl);
   EMG_CUDA(cudaStreamSynchronize(c.stream));
   c.kernel_ms["solve_block"] = total_s * 1e3;
   c.block_initial_res = r0;
+  c.block_floor_res = fl;
 }
 
 int emg_solve_block_dev(emg_context *c, int k, const double *freqs, const double *rhs_dev, double *x_dev,
@@ -1810,6 +1837,56 @@ int emg_spmv_complex_dev(emg_context *c, int k, const double *omegas, const doub
   c->ws->omega_k.upload(omegas, k, c->stream);
   spmm_complex(c->ne, k, c->rp.p, c->ci.p, c->Cv.p, c->Msv.p, c->ws->omega_k.p, x_dev, nullptr, y_dev, false,
                conj_out != 0, c->stream);
+  EMG_API_END
+}
+
+int emg_spmm_layout_dev(emg_context *c, int fp32, int K, int v, int variant, const double *omegas,
+                        const void *x_dev, const void *b_dev, void *y_dev) {
+  EMG_API_BEGIN
+  need(c && omegas && x_dev && b_dev && y_dev, EMG_ERR_ARG, "null argument");
+  need(c->assembled, EMG_ERR_STATE, "operator not assembled");
+  need(K >= 1 && K <= 64, EMG_ERR_ARG, "block width K out of range");
+  use_device(*c);
+  cudaStream_t s = c->stream;
+  c->ws->omega_k.upload(omegas, K, s);
+  SpmmArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = c->ne;
+  a.rp = c->rp.p;
+  a.ci = c->ci.p;
+  a.omega = c->ws->omega_k.p;
+  a.x = x_dev;
+  a.b = b_dev;
+  a.y = y_dev;
+  a.relax_w = 1.0;
+  a.mode = SPMM_RES;
+  bool ok;
+  if (fp32) {
+    // the operator in FP32 (and as packed records) for this call only
+    DBuf<float> vc(c->nnz), vm(c->nnz);
+    DBuf<int4> pk(c->nnz);
+    cvt_d2f(c->nnz, c->Cv.p, vc.p, s);
+    cvt_d2f(c->nnz, c->Msv.p, vm.p, s);
+    pack_records(c->nnz, c->ci.p, vc.p, vm.p, pk.p, s);
+    a.vc = vc.p;
+    a.vm = vm.p;
+    a.pk = pk.p;
+    ok = spmm_layout<float>(K, v, variant, a, s);
+    EMG_CUDA(cudaStreamSynchronize(s));  // the temporaries are freed next
+  } else {
+    a.vc = c->Cv.p;
+    a.vm = c->Msv.p;
+    ok = spmm_layout<double>(K, v, variant, a, s);
+  }
+  if (!ok) fail(EMG_ERR_ARG, "lane layout V=%d variant %d is not available for K=%d", v, variant, K);
+  EMG_API_END
+}
+
+int emg_last_residual_floors(emg_context *c, int k, double *rel) {
+  EMG_API_BEGIN
+  need(c && rel && k >= 0, EMG_ERR_ARG, "null argument");
+  need((size_t)k <= c->block_floor_res.size(), EMG_ERR_STATE, "no block solve of that width yet");
+  std::copy(c->block_floor_res.begin(), c->block_floor_res.begin() + k, rel);
   EMG_API_END
 }
 

@@ -180,6 +180,18 @@ __device__ __forceinline__ void fused_spmm(const SpmmArgs &a) {
       ldv_cg<T, V>(static_cast<const T *>(a.b) + o, bv);
 #pragma unroll
       for (int i = 0; i < V; ++i) out[i] = bv[i] - acc[i];
+    } else if (mode == SPMM_AXJ0) {
+      const T dc = __ldg(static_cast<const T *>(a.l1c) + row);
+      const T dm = a.l1m ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+      T dd[V];
+#pragma unroll
+      for (int i = 0; i < V; ++i) {
+        const T dg = a.l1m ? dc + (T)__ldg(a.omega + cb * V + i) * dm : dc;
+        out[i] = acc[i];
+        dd[i] = (T)a.c1 * acc[i] / dg;
+      }
+      stv<T, V>(static_cast<T *>(a.r) + o, dd);
+      if (a.d) stv<T, V>(static_cast<T *>(a.d) + o, dd);
     } else if (mode == SPMM_ADD) {
       T yo[V];
       ldv_cg<T, V>(y + o, yo);
@@ -207,6 +219,20 @@ __device__ __forceinline__ void fused_spmm(const SpmmArgs &a) {
           rr[i] = bv[i] - acc[i];
           dd[i] = (T)a.c1 * rr[i] / dg;
           out[i] = xo[i] + dd[i];
+        }
+        stv<T, V>(static_cast<T *>(a.r) + o, rr);
+        stv<T, V>(static_cast<T *>(a.d) + o, dd);
+      } else if (mode == SPMM_CHEBK) {
+        T rr[V], dd[V], xo[V], yo[V];
+        ldv_cg<T, V>(static_cast<const T *>(a.b) + o, rr);
+        ldv_cg<T, V>(x + o, xo);
+        ldv_cg<T, V>(y + o, yo);
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+          T dg = two ? dc + w[i] * dm : dc;
+          rr[i] = rr[i] - acc[i];
+          dd[i] = (T)a.c1 * xo[i] + (T)a.c2 * rr[i] / dg;
+          out[i] = yo[i] + dd[i];
         }
         stv<T, V>(static_cast<T *>(a.r) + o, rr);
         stv<T, V>(static_cast<T *>(a.d) + o, dd);

@@ -168,14 +168,24 @@ struct Options {
   int amg_max_coarse = 200;
   int amg_max_levels = 25;
   int amg_relax_times = 1;
-  int smoother_cheb = 1;  // degree-2 Chebyshev (1) or l1-Jacobi (0) in AMS and AMG
+  int smoother_cheb = 1;  // Chebyshev (1) or l1-Jacobi (0) in AMS and AMG
+  int cheb_degree = 2;        // Chebyshev degree of the edge smoother (reference-facing path)
+  // the same in the batched path's AMS: one degree-4 sweep per smoothing
+  // step (measured on the MT topography block of 16 columns at 1.8M edges:
+  // 8.8 s per solve against 9.6 s for two degree-2 sweeps, 11.5 s for one)
+  int block_cheb_degree = 4;
+  int amg_cheb_degree = 2;    // the same on the nodal AMG levels
+  int restrict_j0 = 1;        // nodal restrictions take the fed level's first smoothing step
+  int block_floor_stop = 1;   // block FGMRES columns stop at the rounding floor of their residual
   int gpu_amg = 1;        // nodal AMG setup on the device (1) or on the host (0)
   int block_fp64_fallback = 1;  // batched path: columns the FP32 AMS leaves unconverged finish in FP64
   // batched path accuracy policy: FP32-preconditioned columns iterate to rtol
-  // times this factor (their receiver H error at a given residual is up to
-  // 10x that of an FP64-preconditioned solve), and columns below
-  // block_fp64_below_hz are solved with the FP64 AMS (0: none)
-  double block_fp32_rtol_factor = 0.1;
+  // times this factor, and columns below block_fp64_below_hz are solved with
+  // the FP64 AMS (0: none).  At one relative residual the receiver fields of
+  // different preconditioners differ: on the MT topography block (1.8M
+  // edges, rtol 1e-8) the per-RHS FP64 method's worst receiver H error was
+  // 1.3e-4, the block path's 2.2e-4 at rtol x 0.1 and 4.6e-5 at rtol x 0.01
+  double block_fp32_rtol_factor = 0.01;
   double block_fp64_below_hz = 0;
   // divergence correction after every block solve: x += G phi with phi the
   // vertex potential that makes G^T (b - A x) vanish at interior vertices
@@ -197,7 +207,7 @@ struct Options {
   int block_inner_max_it = 30;
   int block_fcg_mmax = 2;
   int block_fcg_check_every = 5;  // inner iterations between host looks at the column status
-  int block_relax_times = 2;      // edge smoothing sweeps per '0' of the batched path's AMS cycle
+  int block_relax_times = 1;      // edge smoothing sweeps per '0' of the batched path's AMS cycle
   int spmm_tiled = 0;         // edge-column SpMMs gather through per-tile shared memory
   int tiled_smem_kb = 64;     // shared memory budget of one tile
   int verbose = 0;
@@ -259,6 +269,7 @@ struct Context {
   std::map<std::string, double> kernel_ms;
   // per column of the last block solve: ||b - A x0|| / ||b|| of its start
   std::vector<double> block_initial_res;
+  std::vector<double> block_floor_res;  // per column of the last block solve: FP64 rounding floor of its residual
   // rank of each boundary edge among the boundary edges (-1 elsewhere)
   std::vector<int> h_bnd_rank;
   DBuf<int> bnd_rank;

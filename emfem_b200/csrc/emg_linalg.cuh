@@ -30,6 +30,16 @@ enum SpmmMode : int {
   // (0, 1]), fused into the two operator applications it needs:
   SPMM_CHEB1 = 4, // r = b - A x ; d = inv_theta D^-1 r ; y = x + d   (stores r, d)
   SPMM_CHEB2 = 5, // y += c1 d + c2 D^-1 (r - A d)      (x = d gathered, y in place)
+  // a middle step of a Chebyshev smoother of degree > 2 (three-term
+  // recurrence): r' = r - A d ; d' = c1 d + c2 D^-1 r' ; y += d'
+  // (x = d gathered, b = r in, r = r' out (may alias b), d = d' out (not x))
+  SPMM_CHEBK = 6,
+  // restriction that also takes the first smoothing step of the level it
+  // feeds from a zero guess: y = A x (that level's right-hand side b'), and
+  // r = d = c1 b' / D' with D' = l1c + w_c l1m the fed level's l1 diagonal
+  // (l1c/l1m of the args; d may be null), c1 = 1/theta (Chebyshev) or the
+  // l1-Jacobi weight
+  SPMM_AXJ0 = 7,
 };
 
 template <typename T, int V>
@@ -118,13 +128,20 @@ __device__ __forceinline__ void epi_load(const SpmmArgs &a, int row, int cb, boo
   const T *__restrict__ x = static_cast<const T *>(a.x);
   T *y = static_cast<T *>(a.y);
   const int mode = a.mode;
+  const bool cheb = mode == SPMM_CHEB1 || mode == SPMM_CHEB2 || mode == SPMM_CHEBK;
+  // b of SPMM_CHEBK is r, which the same row overwrites: plain load
   if (mode == SPMM_RES || mode == SPMM_JAC || mode == SPMM_CHEB1) ldv<T, V>(static_cast<const T *>(a.b) + o, e.b);
-  if (mode == SPMM_JAC || mode == SPMM_CHEB1 || mode == SPMM_CHEB2) ldv<T, V>(x + o, e.x);
+  if (mode == SPMM_CHEBK) ldv_plain<T, V>(static_cast<const T *>(a.b) + o, e.b);
+  if (mode == SPMM_JAC || cheb) ldv<T, V>(x + o, e.x);
   if (mode == SPMM_CHEB2) ldv<T, V>(static_cast<const T *>(a.r) + o, e.r);
-  if (mode == SPMM_ADD || mode == SPMM_CHEB2) ldv_plain<T, V>(y + o, e.y);
-  if (mode == SPMM_JAC || mode == SPMM_CHEB1 || mode == SPMM_CHEB2) {
+  if (mode == SPMM_ADD || mode == SPMM_CHEB2 || mode == SPMM_CHEBK) ldv_plain<T, V>(y + o, e.y);
+  if (mode == SPMM_JAC || cheb) {
     e.dc = __ldg(static_cast<const T *>(a.l1c) + row);
     e.dm = two ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
+  }
+  if (mode == SPMM_AXJ0) {  // the fed level's diagonal; A itself has one part
+    e.dc = __ldg(static_cast<const T *>(a.l1c) + row);
+    e.dm = a.l1m ? __ldg(static_cast<const T *>(a.l1m) + row) : T(0);
   }
 }
 
@@ -162,6 +179,31 @@ __device__ __forceinline__ void epi_store(const SpmmArgs &a, int row, int cb, co
       rr[i] = e.b[i] - acc[i];
       dd[i] = (T)a.c1 * rr[i] / dg;
       out[i] = e.x[i] + dd[i];
+    }
+    stv<T, V>(static_cast<T *>(a.r) + o, rr);
+    stv<T, V>(static_cast<T *>(a.d) + o, dd);
+    break;
+  }
+  case SPMM_AXJ0: {
+    T dd[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      const T dg = a.l1m ? e.dc + (T)__ldg(a.omega + cb * V + i) * e.dm : e.dc;
+      out[i] = acc[i];
+      dd[i] = (T)a.c1 * acc[i] / dg;
+    }
+    stv<T, V>(static_cast<T *>(a.r) + o, dd);
+    if (a.d) stv<T, V>(static_cast<T *>(a.d) + o, dd);
+    break;
+  }
+  case SPMM_CHEBK: {
+    T rr[V], dd[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      T dg = two ? e.dc + w[i] * e.dm : e.dc;
+      rr[i] = e.b[i] - acc[i];
+      dd[i] = (T)a.c1 * e.x[i] + (T)a.c2 * rr[i] / dg;
+      out[i] = e.y[i] + dd[i];
     }
     stv<T, V>(static_cast<T *>(a.r) + o, rr);
     stv<T, V>(static_cast<T *>(a.d) + o, dd);
@@ -254,6 +296,83 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
 #pragma unroll
     for (int i = 0; i < V; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
   if (!valid || sl != 0) return;
+  epi_store<T, K, V>(a, row, cb, acc, w, two, epi);
+}
+
+// Software-pipelined row SpMM: CL = K / V lanes serve one row (lane j owns
+// column block j), 32 / CL rows per warp.  A row's nonzeros go in chunks of
+// U; the index and value loads of chunk i + 1 are issued right after the x
+// gathers of chunk i, before its FMAs, so the two dependent latencies of a
+// chunk (index load, then gather) overlap with those of its neighbours
+// instead of adding up chunk after chunk.  No warp shuffles: a lane whose row
+// is past the end leaves at once.  Measured on the MT topography edge matrix
+// (1.8M rows, 32 columns) it was never faster than spmm_kernel with packed
+// records over the solver's mix of modes, so the autotuner does not try it;
+// emg_spmm_layout_dev runs it (tests, experiments).
+template <typename T, int K, int V, int U, bool PK>
+__global__ void __launch_bounds__(256) spmm_pipe_kernel(SpmmArgs a) {
+  constexpr int CL = K / V;
+  static_assert(CL <= 32 && (32 % CL) == 0, "bad lane layout");
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int row = gwarp * (32 / CL) + lane / CL;
+  const int cb = lane % CL;
+  if (row >= a.n) return;
+  const T *__restrict__ vc = static_cast<const T *>(a.vc);
+  const T *__restrict__ vm = static_cast<const T *>(a.vm);
+  const T *__restrict__ x = static_cast<const T *>(a.x);
+  const bool two = vm != nullptr;
+  T w[V], acc[V];
+#pragma unroll
+  for (int i = 0; i < V; ++i) {
+    w[i] = two ? (T)__ldg(a.omega + cb * V + i) : T(0);
+    acc[i] = T(0);
+  }
+  EpiIn<T, V> epi;
+  epi_load<T, K, V>(a, row, cb, two, epi);
+  const int kb = __ldg(a.rp + row), ke = __ldg(a.rp + row + 1);
+  int j[U];
+  T c[U], m[U];
+  auto load_chunk = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + u;
+      const bool ok = k < ke;
+      if constexpr (PK) {
+        const int4 rec = ok ? __ldg(a.pk + k) : make_int4(0, 0, 0, 0);
+        j[u] = rec.x;
+        c[u] = (T)__int_as_float(rec.y);
+        m[u] = (T)__int_as_float(rec.z);
+      } else {
+        j[u] = ok ? __ldg(a.ci + k) : 0;
+        c[u] = ok ? __ldg(vc + k) : T(0);
+        m[u] = (ok && two) ? __ldg(vm + k) : T(0);
+      }
+    }
+  };
+  load_chunk(kb);
+  for (int k0 = kb; k0 < ke; k0 += U) {
+    T xv[U][V];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < ke) ldv<T, V>(x + (long)j[u] * K + cb * V, xv[u]);
+      else {
+#pragma unroll
+        for (int i = 0; i < V; ++i) xv[u][i] = T(0);
+      }
+    }
+    T cc[U], mm[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      cc[u] = c[u];
+      mm[u] = m[u];
+    }
+    if (k0 + U < ke) load_chunk(k0 + U);
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int i = 0; i < V; ++i) acc[i] = fma(two ? cc[u] + w[i] * mm[u] : cc[u], xv[u][i], acc[i]);
+  }
   epi_store<T, K, V>(a, row, cb, acc, w, two, epi);
 }
 

@@ -34,6 +34,15 @@ double spmm_algo_bytes(long n, long nnz, int K, int elem, bool two_parts, int mo
 template <typename T>
 void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s);
 
+// one SpMM with a given lane layout (v, nl as in the tuning table: nl > 0 the
+// row-split kernel, -B the row-group kernel, 100 + NL packed records,
+// 200 + U / 300 + U the software-pipelined kernel on arrays / packed
+// records); false when the layout is not legal for (T, K)
+template <typename T>
+bool spmm_layout(int K, int v, int nl, const SpmmArgs &a, cudaStream_t s);
+// FP32 two-part operator as one 16-byte record per nonzero (column, vc, vm, 0)
+void pack_records(long nnz, const int *ci, const float *vc, const float *vm, int4 *out, cudaStream_t s);
+
 // Tiles rows of a host CSR pattern for spmm_tiled: the largest R (a power of
 // two <= r_max, >= 8) whose busiest tile has at most umax_limit distinct
 // columns.  Returns false (tp untouched) when no such R exists.
@@ -127,5 +136,10 @@ void cscale(int n, int K, const double *w, const double *scale, double *v, cudaS
 void cupdate(int n, int K, int J, const double *Z, long stride, const double *y, double *x, cudaStream_t s);
 // out[c] += ||x_c||^2 over complex columns
 void cnorm2(int n, int K, const double *x, double *out, cudaStream_t s);
+// out[c] += || |b_c| + (|C| + w_c |Ms|) |x_c| ||^2 for K complex columns (K
+// divides 32): u times its root bounds the rounding error of a computed
+// residual b - (C + i w Ms) x, the floor below which no iteration can push it
+void abs_bound2(int n, int K, const int *rp, const int *ci, const double *Cv, const double *Mv, const double *omega,
+                const double *x, const double *b, double *out, cudaStream_t s);
 
 }  // namespace emg

@@ -178,12 +178,6 @@ struct StageClock {
   }
 };
 
-__global__ void pack_records_kernel(long nnz, const int *__restrict__ ci, const float *__restrict__ vc,
-                                    const float *__restrict__ vm, int4 *__restrict__ out) {
-  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (k < nnz) out[k] = make_int4(ci[k], __float_as_int(vc[k]), __float_as_int(vm[k]), 0);
-}
-
 template <typename T>
 void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_ref) {
   cudaStream_t s = c.stream;
@@ -201,6 +195,9 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   ams.relax_w = c.opt.ams_relax_weight;
   ams.amg_relax_times = c.opt.amg_relax_times;
   ams.cheb = c.opt.smoother_cheb;
+  ams.cheb_degree = per_frequency ? c.opt.cheb_degree : c.opt.block_cheb_degree;
+  ams.amg_cheb_degree = c.opt.amg_cheb_degree;
+  ams.restrict_j0 = c.opt.restrict_j0 != 0;
   ams.two = !per_frequency;
   ams.use_graphs = c.opt.graphs != 0;
   ams.fused = c.opt.ams_fused != 0;
@@ -248,9 +245,7 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   // packed variant (the autotuner decides whether it is used)
   if (sizeof(T) == 4 && !per_frequency) {
     ams.Bpk.alloc(c.nnz);
-    pack_records_kernel<<<g, 256, 0, s>>>(c.nnz, c.ci.p, (const float *)ams.B.vc.p, (const float *)ams.B.vm.p,
-                                          ams.Bpk.p);
-    EMG_LAUNCH_CHECK();
+    pack_records(c.nnz, c.ci.p, (const float *)ams.B.vc.p, (const float *)ams.B.vm.p, ams.Bpk.p, s);
   } else {
     ams.Bpk.release();
   }
@@ -454,6 +449,8 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
   er.alloc((size_t)ne * K);
   ex2.alloc((size_t)ne * K);
   ed.alloc((size_t)ne * K);
+  if (cheb && cheb_degree > 2) ed2.alloc((size_t)ne * K);
+  else ed2.release();
   gtmp.alloc((size_t)nv * K);
   for (int sp = 0; sp < NSUB; ++sp) {
     Sub &S = sub[sp];
@@ -463,7 +460,9 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
     wr[sp].clear();
     wx2[sp].clear();
     wd[sp].clear();
+    wd2[sp].clear();
     wd[sp].resize(L + 1);
+    wd2[sp].resize(L + 1);
     wb[sp].resize(L + 1);
     wx[sp].resize(L + 1);
     wr[sp].resize(L + 1);
@@ -476,6 +475,7 @@ void Ams<T>::ensure_workspace(cudaStream_t s) {
         wr[sp][l].alloc(n);
         wx2[sp][l].alloc(n);
         wd[sp][l].alloc(n);
+        if (cheb && amg_cheb_degree > 2) wd2[sp][l].alloc(n);
       }
     }
   }
@@ -600,23 +600,39 @@ static SpmmArgs level_args(const DCsr<T> &A, int mode, const double *omega, doub
   return a;
 }
 
-// Chebyshev coefficients for degree 2 on D^-1 A with D the l1 row sums:
-// the spectrum lies in (0, 1], smoothed interval [1/30, 1]
-struct Cheb2 {
-  double inv_theta, c1, c2;
-  Cheb2() {
+// Chebyshev smoothing of degree m on D^-1 A with D the l1 row sums: the
+// spectrum lies in (0, 1], the smoothed interval is [1/30, 1].  Three-term
+// recurrence (Saad, Iterative Methods for Sparse Linear Systems, 2nd ed.,
+// Alg. 12.1): theta, delta the interval's centre and half-width, sigma =
+// theta / delta, rho_0 = 1 / sigma, rho_k = 1 / (2 sigma - rho_{k-1});
+// d_0 = D^-1 r_0 / theta, then r_k = r_{k-1} - A d_{k-1},
+// d_k = rho_k rho_{k-1} d_{k-1} + (2 rho_k / delta) D^-1 r_k, x += d_k.
+struct ChebCoef {
+  double inv_theta;
+  double c1[8], c2[8];  // step k = 1 .. m-1
+  explicit ChebCoef(int m) {
     const double lmax = 1.0, lmin = lmax / 30.0;
-    const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), s1 = th / de;
-    const double r0 = 1.0 / s1, r1 = 1.0 / (2.0 * s1 - r0);
+    const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sg = th / de;
     inv_theta = 1.0 / th;
-    c1 = r1 * r0;
-    c2 = 2.0 * r1 / de;
+    double rho = 1.0 / sg;
+    for (int k = 1; k < m && k < 8; ++k) {
+      const double rn = 1.0 / (2.0 * sg - rho);
+      c1[k] = rn * rho;
+      c2[k] = 2.0 * rn / de;
+      rho = rn;
+    }
   }
 };
 
+static const ChebCoef &cheb_coef(int m) {
+  static const ChebCoef tab[7] = {ChebCoef(2), ChebCoef(2), ChebCoef(2), ChebCoef(3),
+                                  ChebCoef(4), ChebCoef(5), ChebCoef(6)};
+  return tab[std::min(std::max(m, 2), 6)];
+}
+
 template <typename T>
-T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b, T *rbuf, T *dbuf,
-                  bool zero_guess, const char *bin, cudaStream_t s) {
+T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b, T *rbuf, T *dbuf, T *dbuf2,
+                  bool zero_guess, const char *bin, cudaStream_t s, bool started) {
   const bool edge = A == nullptr;
   const T *l1c = edge ? B.l1c.p : A->l1c.p;
   const T *l1m = edge ? (two ? B.l1m.p : nullptr) : A->l1m.p;
@@ -645,25 +661,39 @@ T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b,
   };
   if (!cheb) {
     if (zero_guess) {
-      emit_jac0(n, b, l1c, l1m, relax_w, cur, nullptr, s);
+      if (!started) emit_jac0(n, b, l1c, l1m, relax_w, cur, nullptr, s);
       return cur;
     }
     run(SPMM_JAC, cur, b, oth, nullptr, nullptr, 0, 0);
     return oth;
   }
-  static const Cheb2 ch;
+  const int m = std::min(std::max(edge ? cheb_degree : amg_cheb_degree, 2), 6);
+  if (m > 2 && !dbuf2) fail(EMG_ERR_STATE, "Chebyshev degree %d without its second direction buffer", m);
+  const ChebCoef &ch = cheb_coef(m);
+  T *y = zero_guess ? cur : oth;
+  const T *rprev;  // r_{k-1}: b itself after a zero start, else rbuf
   if (zero_guess) {
-    emit_jac0(n, b, l1c, l1m, ch.inv_theta, cur, dbuf, s);
-    run(SPMM_CHEB2, dbuf, nullptr, cur, const_cast<T *>(b), nullptr, ch.c1, ch.c2);
-    return cur;
+    if (!started) emit_jac0(n, b, l1c, l1m, ch.inv_theta, cur, dbuf, s);
+    rprev = b;
+  } else {
+    run(SPMM_CHEB1, cur, b, oth, rbuf, dbuf, ch.inv_theta, 0);
+    rprev = rbuf;
   }
-  run(SPMM_CHEB1, cur, b, oth, rbuf, dbuf, ch.inv_theta, 0);
-  run(SPMM_CHEB2, dbuf, nullptr, oth, rbuf, nullptr, ch.c1, ch.c2);
-  return oth;
+  T *dA = dbuf, *dB = dbuf2;
+  for (int k = 1; k < m; ++k) {
+    if (k + 1 == m) {
+      run(SPMM_CHEB2, dA, nullptr, y, const_cast<T *>(rprev), nullptr, ch.c1[k], ch.c2[k]);
+    } else {
+      run(SPMM_CHEBK, dA, rprev, y, rbuf, dB, ch.c1[k], ch.c2[k]);
+      rprev = rbuf;
+      std::swap(dA, dB);
+    }
+  }
+  return y;
 }
 
 template <typename T>
-void Ams<T>::vcycle(int sp, int l, cudaStream_t s) {
+void Ams<T>::vcycle(int sp, int l, cudaStream_t s, bool started) {
   Sub &S = sub[sp];
   const int L = (int)S.lv.size();
   if (fused && !rec && l == fused_from[sp] && l < L) {
@@ -684,17 +714,31 @@ void Ams<T>::vcycle(int sp, int l, cudaStream_t s) {
   T *cur = (swaps & 1) ? wx2[sp][l].p : wx[sp][l].p;
   T *oth = (swaps & 1) ? wx[sp][l].p : wx2[sp][l].p;
   const T *b = wb[sp][l].p;
-  T *r = wr[sp][l].p, *d = wd[sp][l].p;
+  T *r = wr[sp][l].p, *d = wd[sp][l].p, *d2 = wd2[sp][l].p;
   for (int it = 0; it < amg_relax_times; ++it) {
-    T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, it == 0, bin, s);
+    T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, d2, it == 0, bin, s, started && it == 0);
     if (res != cur) std::swap(cur, oth);
   }
   emit_spmm(level_args<T>(lv.A, SPMM_RES, omega.p, relax_w, cur, b, r), lv.nnzA, bin, s);
-  emit_spmm(level_args<T>(lv.R, SPMM_AX, nullptr, 1.0, r, nullptr, wb[sp][l + 1].p), lv.nnzR, bin, s);
-  vcycle(sp, l + 1, s);
+  // the restriction to a level (not the coarsest) also takes that level's
+  // first zero-guess smoothing step, into the buffer vcycle(l + 1) starts in
+  SpmmArgs ra = level_args<T>(lv.R, SPMM_AX, nullptr, 1.0, r, nullptr, wb[sp][l + 1].p);
+  const bool j0 = restrict_j0 && l + 1 < L;
+  if (j0) {
+    const DCsr<T> &An = S.lv[l + 1].A;
+    ra.mode = SPMM_AXJ0;
+    ra.omega = omega.p;
+    ra.l1c = An.l1c.p;
+    ra.l1m = An.l1m.p;
+    ra.r = (swaps & 1) ? wx2[sp][l + 1].p : wx[sp][l + 1].p;
+    ra.d = cheb ? wd[sp][l + 1].p : nullptr;
+    ra.c1 = cheb ? cheb_coef(amg_cheb_degree).inv_theta : relax_w;
+  }
+  emit_spmm(ra, lv.nnzR, bin, s);
+  vcycle(sp, l + 1, s, j0);
   emit_spmm(level_args<T>(lv.P, SPMM_ADD, nullptr, 1.0, wx[sp][l + 1].p, nullptr, cur), lv.nnzP, bin, s);
   for (int it = 0; it < amg_relax_times; ++it) {
-    T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, false, bin, s);
+    T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, d2, false, bin, s);
     if (res != cur) std::swap(cur, oth);
   }
 }
@@ -850,7 +894,7 @@ void Ams<T>::apply_eager(const T *b, T *x, cudaStream_t s) {
     const char ch = cycle[ci];
     if (ch == '0') {
       for (int it = 0; it < relax_times; ++it) {
-        T *res = smooth(nullptr, nnzB, ne, cur, oth, b, er.p, ed.p, zero, bin, s);
+        T *res = smooth(nullptr, nnzB, ne, cur, oth, b, er.p, ed.p, ed2.p, zero, bin, s);
         if (res != cur) std::swap(cur, oth);
         zero = false;
       }
@@ -1129,7 +1173,16 @@ struct GmDev {
   const double *bnorm;
   double *scale;   // K: divisor of the next basis vector (0: column finished)
   int *status;     // [0] columns still iterating, [1] 1 + first column with NaN/Inf
+  const double *tol;  // K: absolute stopping tolerance of the residual norm
 };
+
+// per column: tol = max(rtol ||b||, u || |b| + |A| |x| ||), u the FP64 unit
+// roundoff; below the second term the computed residual is rounding noise
+__global__ void gm_tol_kernel(int K, double rtol, const double *__restrict__ bnorm,
+                              const double *__restrict__ bound2, double *__restrict__ tol) {
+  const int c = threadIdx.x;
+  if (c < K) tol[c] = fmax(rtol * bnorm[c], 0x1p-53 * sqrt(bound2[c]));
+}
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -1148,7 +1201,7 @@ __global__ void gm_start_kernel(int K, int J, const double *__restrict__ nrm2, d
   if (c < K) {
     const double beta = sqrt(nrm2[c]);
     if (!isfinite(beta)) atomicCAS(st.status + 1, 0, c + 1);
-    if (beta <= rtol * st.bnorm[c]) st.conv[c] = 1;
+    if (beta <= st.tol[c]) st.conv[c] = 1;
     if (stall > 0 && prev[c] > 0 && beta > stall * prev[c]) st.conv[c] = 1;
     prev[c] = beta;
     const bool cv = st.conv[c] != 0 || !isfinite(beta);
@@ -1210,7 +1263,7 @@ __global__ void gm_givens_kernel(int K, int J, int j, const double2 *__restrict_
       g[j] = zmul(cs[j], gj);
       st.jc[c] = j + 1;
       st.colits[c]++;
-      if (zabs(g[j + 1]) <= rtol * st.bnorm[c] || hnext == 0.0 || !isfinite(hnext)) st.done[c] = 1;
+      if (zabs(g[j + 1]) <= st.tol[c] || hnext == 0.0 || !isfinite(hnext)) st.done[c] = 1;
       act = !st.done[c];
     }
   }
@@ -1288,6 +1341,9 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   snd.alloc((size_t)k * J * 2);
   gd.alloc((size_t)k * (J + 1) * 2);
   ints.alloc((size_t)4 * k + 2);
+  tol.alloc(k);
+  bound2.alloc(k);
+  const bool use_floor = floor_stop && !real_form;
   if (!h_status.p) EMG_CUDA(cudaMallocHost((void **)&h_status.p, 2 * sizeof(int)));
   GmDev gs;
   gs.H = (double2 *)Hd.p;
@@ -1301,6 +1357,7 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   gs.status = ints.p + 4 * k;
   gs.bnorm = bnd.p;
   gs.scale = scale.p;
+  gs.tol = tol.p;
   ints.zero(s);
   prevb.alloc(k);
   prevb.zero(s);
@@ -1321,6 +1378,11 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
     if (bnorm[col] == 0) conv0[col] = 1;
   }
   bnd.upload(bnorm, s);
+  {
+    std::vector<double> t0(k);
+    for (int col = 0; col < k; ++col) t0[col] = rtol * bnorm[col];
+    tol.upload(t0, s);
+  }
   EMG_CUDA(cudaMemcpyAsync(gs.conv, conv0.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
   st.initial_res.assign(k, 1.0);
   if (use_guess) {
@@ -1361,10 +1423,19 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
     if (h_status.p[1]) fail(EMG_DIVERGED_NANORINF, "FGMRES: NaN or Inf in the residual of column %d", h_status.p[1] - 1);
     return h_status.p[0];
   };
+  auto floor_scale = [&]() {
+    bound2.zero(s);
+    abs_bound2(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, bound2.p, s);
+  };
   while (total < maxit) {
     spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, r.p, true, real_form, s);
     nrm.zero(s);
     cnorm2(n, k, r.p, nrm.p, s);
+    if (use_floor) {
+      floor_scale();
+      gm_tol_kernel<<<1, 1024, 0, s>>>(k, rtol, bnd.p, bound2.p, tol.p);
+      EMG_LAUNCH_CHECK();
+    }
     gm_start_kernel<<<1, 1024, 0, s>>>(k, J, nrm.p, rtol, stall_factor, prevb.p, gs);
     EMG_LAUNCH_CHECK();
     if (read_status() == 0) break;
@@ -1402,8 +1473,12 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   spmm_complex(n, k, c.rp.p, c.ci.p, c.Cv.p, c.Msv.p, omega.p, x, b, r.p, true, real_form, s);
   nrm.zero(s);
   cnorm2(n, k, r.p, nrm.p, s);
-  std::vector<double> tr(k);
+  std::vector<double> tr(k), fb(k, 0.0);
   nrm.download(tr.data(), k, s);
+  if (use_floor) {
+    floor_scale();
+    bound2.download(fb.data(), k, s);
+  }
   st.col_its.assign(k, 0);
   EMG_CUDA(cudaMemcpyAsync(st.col_its.data(), gs.colits, sizeof(int) * k, cudaMemcpyDeviceToHost, s));
   EMG_CUDA(cudaEventRecord(e1, s));
@@ -1415,9 +1490,14 @@ int Fgmres::solve(Context &c, const double *b, double *x, bool use_guess, double
   st.seconds = ms * 1e-3;
   st.true_res.assign(k, 0.0);
   st.converged.assign(k, 0);
+  st.floor_res.assign(k, 0.0);
+  st.at_floor.assign(k, 0);
   for (int col = 0; col < k; ++col) {
     st.true_res[col] = bnorm[col] > 0 ? std::sqrt(tr[col]) / bnorm[col] : 0.0;
     st.converged[col] = st.true_res[col] <= rtol * 1.0000001 || bnorm[col] == 0 ? 1 : 0;
+    st.floor_res[col] = bnorm[col] > 0 ? 0x1p-53 * std::sqrt(fb[col]) / bnorm[col] : 0.0;
+    // above rtol but within twice the rounding floor: no iteration can do better
+    st.at_floor[col] = !st.converged[col] && use_floor && st.true_res[col] <= 2.0 * st.floor_res[col] ? 1 : 0;
   }
   st.outer_its = total;
   return total;

@@ -120,7 +120,10 @@ struct Ams {
   int relax_times = 1;
   double relax_w = 1.0;
   int amg_relax_times = 1;
-  int cheb = 1;                    // 1: degree-2 Chebyshev smoothing, 0: l1-Jacobi
+  int cheb = 1;                    // 1: Chebyshev smoothing, 0: l1-Jacobi
+  int cheb_degree = 2;             // operator applications per edge smoothing sweep
+  int amg_cheb_degree = 2;         // the same on the nodal levels
+  bool restrict_j0 = true;         // restrictions take the fed level's first smoothing step
   bool use_graphs = true;          // replay each application as one CUDA graph
   bool split_gradient = false;     // last '1' of the cycle returned as potential gphi()
   // each nodal V-cycle as one cooperative launch (emg_fused.cu) instead of
@@ -146,8 +149,8 @@ struct Ams {
   DBuf<int> cslot;                 // K, coarse-inverse index per column
   std::vector<double> h_omega;
   // workspace
-  DBuf<T> er, ex2, ed;
-  std::vector<DBuf<T>> wb[NSUB], wx[NSUB], wr[NSUB], wx2[NSUB], wd[NSUB];
+  DBuf<T> er, ex2, ed, ed2;        // ed2, wd2: second direction buffers (degree > 2)
+  std::vector<DBuf<T>> wb[NSUB], wx[NSUB], wr[NSUB], wx2[NSUB], wd[NSUB], wd2[NSUB];
 
   void set_columns(const std::vector<double> &col_omega, cudaStream_t s);
   void apply(const T *b, T *x, cudaStream_t s);
@@ -159,7 +162,9 @@ struct Ams {
   void spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s);
   size_t device_bytes() const;
 
-  void vcycle(int sp, int l, cudaStream_t s);
+  // started: the restriction that fed level l already took its first
+  // zero-guess smoothing step (SPMM_AXJ0)
+  void vcycle(int sp, int l, cudaStream_t s, bool started = false);
   // runs subspace sp's V-cycle: the levels with at least fused_rows rows
   // step by step, the rest as one fused launch
   void run_vcycle(int sp, cudaStream_t s);
@@ -177,8 +182,8 @@ struct Ams {
   void emit_coarse(int sp, const T *b, T *x, cudaStream_t s);
   // one smoothing application on operator A (edge B when A == nullptr);
   // returns the buffer holding the result (cur, or oth after a swap)
-  T *smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b, T *rbuf, T *dbuf, bool zero_guess,
-            const char *bin, cudaStream_t s);
+  T *smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b, T *rbuf, T *dbuf, T *dbuf2,
+            bool zero_guess, const char *bin, cudaStream_t s, bool started = false);
   void ensure_workspace(cudaStream_t s);
   int ws_K = 0;
 };
@@ -236,7 +241,10 @@ struct SolveStats {
   std::vector<int> col_its;
   std::vector<int> converged;
   std::vector<double> initial_res;  // per column: ||b - A x0|| / ||b|| of the start used
+  std::vector<double> floor_res;    // per column: the FP64 rounding floor of the relative residual at exit
+  std::vector<int> at_floor;        // per column: stopped at that floor above rtol
   double seconds = 0;
+  bool settled(int c) const { return converged[c] || (c < (int)at_floor.size() && at_floor[c]); }
 };
 
 // Batched FGMRES(restart) on k complex columns (FP64):
@@ -252,6 +260,11 @@ struct Fgmres {
   PinnedWord h_status;
   DBuf<double> prevb;                  // residual norm at the previous restart, per column
   double stall_factor = 0;             // > 0: stop a column whose residual fell less than this over a cycle
+  // complex form only: a column also stops once its residual reaches the
+  // rounding floor of its own computation, u || |b| + |A| |x| || (recomputed
+  // at every restart), when that lies above rtol ||b||
+  bool floor_stop = false;
+  DBuf<double> tol, bound2;            // per column: absolute stopping tolerance, the floor's squared scale
   int solve(Context &c, const double *b, double *x, bool use_guess, double rtol, int maxit, bool real_form,
             const std::function<void(const double *, double *)> &precond, SolveStats &st);
 };

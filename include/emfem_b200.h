@@ -27,6 +27,11 @@ extern "C" {
 #define EMG_DIVERGED_ITS (-6)      /* Krylov hit max_it before rtol            */
 #define EMG_DIVERGED_NANORINF (-7) /* NaN or Inf in a residual                 */
 #define EMG_ERR_OPTION (-8)        /* unknown or malformed option              */
+/* a block-solve column whose residual reached the FP64 rounding floor of its
+ * own computation, u || |b| + |A||x| || (u = 2^-53), above rtol ||b||: no
+ * iteration can lower it further (emg_last_residual_floors gives the floor;
+ * no counterpart in the reference, whose KSP runs on to max_it there) */
+#define EMG_STOPPED_AT_FLOOR 1
 
 /* anisotropy forms, src/em_defs.h:37 */
 #define EMG_ISOTROPIC 0
@@ -46,7 +51,7 @@ typedef struct emg_context emg_context;
 typedef struct emg_solve_info {
   int outer_its;        /* FGMRES iterations                                 */
   int inner_its;        /* total FCG iterations (both real blocks)           */
-  int reason;           /* 0 converged, EMG_DIVERGED_* otherwise             */
+  int reason;           /* 0 converged, EMG_STOPPED_AT_FLOOR, EMG_DIVERGED_* */
   double true_rel_res;  /* ||b - A x|| / ||b|| recomputed in FP64 at exit    */
   double seconds;       /* device time of the solve                          */
 } emg_solve_info;
@@ -378,6 +383,16 @@ int emg_warm_start_losses(emg_context *ctx, double *loss, double *loss_interp);
  * real-form operator of matshell_mult_a) for k complex columns. */
 int emg_spmv_complex_dev(emg_context *ctx, int k, const double *omegas_host, const double *x_dev,
                          double *y_dev, int conj_out);
+/* y = b - (C + w_c Ms) x on K real columns (row-major n_edges x K, x, b
+ * and y float when fp32 != 0, else double; omegas_host holds the K column
+ * shifts w_c) with the SpMM lane layout (v, variant) forced instead of the
+ * autotuner's choice: v columns per vector load; variant > 0 and < 100 the
+ * row-split kernel with that many lanes per row, -B the row-group kernel,
+ * 100 + NL / 300 + U packed 16-byte records (fp32 only), 200 + U the
+ * software-pipelined kernel with chunks of U nonzeros.  EMG_ERR_ARG for a
+ * layout not built for K.  Tests every kernel the autotuner can pick. */
+int emg_spmm_layout_dev(emg_context *ctx, int fp32, int K, int v, int variant, const double *omegas_host,
+                        const void *x_dev, const void *b_dev, void *y_dev);
 /* the nodal AMG hierarchy of AMS subspace sp (0 gradient, 1-3 Pi_x/y/z, 4 the
  * vector space) of the assembled operators, built on the device (gpu != 0)
  * or by the host build, for reference frequency w_ref: per level 5 values
@@ -388,6 +403,10 @@ int emg_amg_levels(emg_context *ctx, int sp, int gpu, double w_ref, int max_rows
  * ||b - A x0|| / ||b|| of the start it used (1 for a zero start, also where
  * a guess was worse than zero and was dropped) */
 int emg_last_initial_residuals(emg_context *ctx, int k, double *rel);
+/* per column of the last emg_solve_block(_dev): u || |b| + |A||x| || / ||b||,
+ * the relative residual below which the computed FP64 residual is rounding
+ * noise (u = 2^-53, |.| entrywise); 0 with -emg_block_floor_stop 0 */
+int emg_last_residual_floors(emg_context *ctx, int k, double *rel);
 /* per-kernel device timing of the last call of each kind (ms) */
 int emg_last_kernel_ms(emg_context *ctx, const char *name, double *ms);
 int emg_stream_synchronize(emg_context *ctx);

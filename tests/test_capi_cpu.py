@@ -75,8 +75,15 @@ def test_solver_extension_options():
                        "emg_fused_blocks_per_sm": 2, "emg_spmm_tiled": 1, "emg_tiled_smem_kb": 32}
         for ct in (1, 3, 5, 7, 11, 13):
             c.process_options("-B_pc_hypre_ams_cycle_type %d" % ct)
+        assert c.get_option("emg_restrict_smooth") == 1
+        c.process_options("-emg_restrict_smooth 0")
+        assert c.get_option("emg_restrict_smooth") == 0
+        c.process_options("-emg_cheb_degree 3 -emg_block_cheb_degree 4 -emg_amg_cheb_degree 6")
+        assert [c.get_option(k) for k in ("emg_cheb_degree", "emg_block_cheb_degree", "emg_amg_cheb_degree")] == \
+            [3, 4, 6]
         for bad in ("-emg_block_inner_max_it 0", "-emg_block_inner_rtol 0", "-emg_block_fcg_mmax 31",
-                    "-emg_tiled_smem_kb 300", "-B_pc_hypre_ams_cycle_type 14"):
+                    "-emg_tiled_smem_kb 300", "-B_pc_hypre_ams_cycle_type 14", "-emg_cheb_degree 1",
+                    "-emg_block_cheb_degree 7", "-emg_amg_cheb_degree 0"):
             with pytest.raises(E.EMGError) as ei:
                 c.process_options(bad)
             assert ei.value.code == E.api.EMG_ERR_OPTION

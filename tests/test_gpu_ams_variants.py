@@ -24,6 +24,12 @@ to 1e-6 of its largest entry.
 3. The same bar with the edge-column SpMMs tiled (x rows of each row tile
 staged once in shared memory), with the default 64 KB and with small tiles
 (16 KB: more, shorter tiles).
+
+4. The same bar with Chebyshev smoothers of degree 3 to 5 (the three-term
+recurrence's middle steps) on the edges of both solvers and on the nodal
+levels, stepwise and in the fused V-cycle; and with each nodal restriction
+taking the fed level's first smoothing step (the default) or leaving it to
+its own launch, for Chebyshev and l1-Jacobi smoothing.
 """
 
 import numpy as np
@@ -92,7 +98,14 @@ def _direct(rp, ci, Cv, Mv, sr, si):
                                    "-emg_spmm_tiled 1",
                                    "-emg_spmm_tiled 1 -emg_tiled_smem_kb 16",
                                    "-emg_fp32_cycle 0201 -B_pc_hypre_ams_cycle_type 7 -emg_fused_vcycle 1 "
-                                   "-emg_fused_rows 400"])
+                                   "-emg_fused_rows 400",
+                                   "-emg_block_cheb_degree 3 -emg_block_relax_times 1 -emg_cheb_degree 4 "
+                                   "-emg_amg_cheb_degree 3",
+                                   "-emg_block_cheb_degree 5 -emg_amg_cheb_degree 4 -emg_fused_vcycle 1 "
+                                   "-emg_fused_rows 400",
+                                   "-emg_restrict_smooth 0",
+                                   "-emg_restrict_smooth 0 -emg_smoother l1jacobi",
+                                   "-emg_smoother l1jacobi"])
 def test_pi_vector_space_cycles(mt_small, extra):
     prob = mt_small
     bg = mg.background_model(prob.mesh, prob.model)
