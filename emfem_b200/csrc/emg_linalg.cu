@@ -21,7 +21,7 @@ constexpr bool spmm_legal() {
   return (K % V) == 0 && (K / V) * NL <= 32 && (32 % ((K / V) * NL)) == 0 && sizeof(T) * V <= 16;
 }
 
-template <typename T, int K, int V, int NL, bool PK = false>
+template <typename T, int K, int V, int NL, bool PK = false, int MINB = 1>
 void spmm_launch(const SpmmArgs &a, cudaStream_t s) {
   constexpr int G = NL * (K / V);
   constexpr int RPW = 32 / G;
@@ -29,7 +29,15 @@ void spmm_launch(const SpmmArgs &a, cudaStream_t s) {
   long threads = warps * 32;
   unsigned grid = (unsigned)((threads + 255) / 256);
   if (grid == 0) return;
-  spmm_kernel<T, K, V, NL, PK><<<grid, 256, 0, s>>>(a);
+  spmm_kernel<T, K, V, NL, PK, MINB><<<grid, 256, 0, s>>>(a);
+}
+
+// register-capped row-split kernel (nl = 400 + NL packed records, 500 + NL
+// index and value arrays): 4 blocks of 256 threads per SM; FP32, K >= 16
+template <typename T, int K, int V, int NL, bool PK>
+SpmmFn spmm_pick_capped() {
+  if constexpr (spmm_legal<T, K, V, NL>() && sizeof(T) == 4 && K >= 16) return &spmm_launch<T, K, V, NL, PK, 4>;
+  else return nullptr;
 }
 
 // row-group kernel (spmm_rows_kernel): nl = -B selects it with B gathers in
@@ -91,6 +99,10 @@ SpmmFn spmm_pick_nl(int nl) {
   case 101: return spmm_pick_packed<T, K, V, 1>();
   case 102: return spmm_pick_packed<T, K, V, 2>();
   case 104: return spmm_pick_packed<T, K, V, 4>();
+  case 401: return spmm_pick_capped<T, K, V, 1, true>();
+  case 402: return spmm_pick_capped<T, K, V, 2, true>();
+  case 501: return spmm_pick_capped<T, K, V, 1, false>();
+  case 502: return spmm_pick_capped<T, K, V, 2, false>();
   case 204: return spmm_pipe_pick<T, K, V, 4, false>();
   case 208: return spmm_pipe_pick<T, K, V, 8, false>();
   case 304: return spmm_pipe_pick<T, K, V, 4, true>();
@@ -139,7 +151,9 @@ std::string SpmmTuner::report() const {
        << std::get<2>(kv.first) << " rows class " << (std::get<3>(kv.first) >> 1) << ": V=" << kv.second.first
        << (std::get<3>(kv.first) & 1 ? " (packed records available)" : "")
        << (kv.second.second < 0 ? " rows kernel B="
-                                : (kv.second.second > 300   ? " packed pipelined U="
+                                : (kv.second.second > 500   ? " register-capped NL="
+                                   : kv.second.second > 400 ? " packed register-capped NL="
+                                   : kv.second.second > 300 ? " packed pipelined U="
                                    : kv.second.second > 200 ? " pipelined U="
                                    : kv.second.second > 100 ? " packed NL="
                                                             : " NL="))
@@ -194,8 +208,8 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
       // then ran 17% slower over the solver's mix of smoothing modes.
       std::vector<std::pair<int, int>> cand;
       for (int v : {1, 2, 4})
-        for (int nl : {1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104}) {
-          if (nl > 100 && !packed) continue;
+        for (int nl : {1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104, 401, 402, 501, 502}) {
+          if (((nl > 100 && nl < 200) || (nl > 400 && nl < 500)) && !packed) continue;
           if (spmm_fn<T>(K, v, nl)) cand.push_back({v, nl});
         }
       // two interleaved passes, each candidate's best: one slow sample (a
@@ -289,7 +303,7 @@ template <typename T>
 bool spmm_layout(int K, int v, int nl, const SpmmArgs &a, cudaStream_t s) {
   SpmmFn f = spmm_fn<T>(K, v, nl);
   if (!f) return false;
-  const bool packed_variant = (nl > 100 && nl < 200) || nl > 300;
+  const bool packed_variant = (nl > 100 && nl < 200) || (nl > 300 && nl < 400) || (nl > 400 && nl < 500);
   if (packed_variant && (a.pk == nullptr || a.vm == nullptr)) return false;
   if (a.n > 0) f(a, s);
   EMG_LAUNCH_CHECK();
@@ -322,7 +336,7 @@ double spmm_algo_bytes(long n, long nnz, int K, int elem, bool two_parts, int mo
   if (mode == SPMM_ADD) b += vec;
   if (mode == SPMM_CHEB1) b += 3.0 * vec + (double)n * elem * (two_parts ? 2 : 1);   // b, x-row in; r, d out
   if (mode == SPMM_CHEB2) b += 2.0 * vec + (double)n * elem * (two_parts ? 2 : 1);   // r, y-row in
-  if (mode == SPMM_CHEBK) b += 5.0 * vec + (double)n * elem * (two_parts ? 2 : 1);   // r, d-row, y in; r, d out
+  if (mode == SPMM_CHEBK) b += 4.0 * vec + (double)n * elem * (two_parts ? 2 : 1);   // r, y in; r, d out
   if (mode == SPMM_AXJ0) b += 2.0 * vec + (double)n * elem * 2;                      // r, d out; fed diagonal
   return b;
 }

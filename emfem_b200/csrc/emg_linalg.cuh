@@ -227,8 +227,10 @@ __device__ __forceinline__ void spmm_epilogue(const SpmmArgs &a, int row, int cb
   epi_store<T, K, V>(a, row, cb, acc, w, two, e);
 }
 
-template <typename T, int K, int V, int NL, bool PK = false>
-__global__ void __launch_bounds__(256) spmm_kernel(SpmmArgs a) {
+// MINB > 1 caps the registers so that MINB blocks of 256 threads fit on an SM
+// (more warps in flight for the load-latency-bound gathers, a few spills)
+template <typename T, int K, int V, int NL, bool PK = false, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) spmm_kernel(SpmmArgs a) {
   constexpr int CL = K / V;
   constexpr int G = NL * CL;
   static_assert(G <= 32 && (32 % G) == 0, "bad lane layout");

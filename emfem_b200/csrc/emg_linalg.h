@@ -37,7 +37,8 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s);
 // one SpMM with a given lane layout (v, nl as in the tuning table: nl > 0 the
 // row-split kernel, -B the row-group kernel, 100 + NL packed records,
 // 200 + U / 300 + U the software-pipelined kernel on arrays / packed
-// records); false when the layout is not legal for (T, K)
+// records, 400 + NL / 500 + NL the register-capped row-split kernel on packed
+// records / arrays); false when the layout is not legal for (T, K)
 template <typename T>
 bool spmm_layout(int K, int v, int nl, const SpmmArgs &a, cudaStream_t s);
 // FP32 two-part operator as one 16-byte record per nonzero (column, vc, vm, 0)

@@ -20,7 +20,7 @@ import emfem_b200 as E
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104, 204, 208, 304, 308]
+VARIANTS = [1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104, 204, 208, 304, 308, 401, 402, 501, 502]
 
 
 @pytest.fixture(scope="module")
@@ -73,8 +73,11 @@ def test_every_layout_matches_float64(edge_operator, fp32, K):
             err = (np.abs(y.double().cpu().numpy() - ref) / scale).max()
             assert err <= tol, (v, var, err)
             ran.append((v, var))
-    # the pipelined and (FP32) packed kernels are among the layouts checked
+    # the pipelined and (FP32) packed and register-capped kernels are among
+    # the layouts checked
     assert any(var in (204, 208) for _, var in ran)
     if fp32:
         assert any(var in (304, 308) for _, var in ran)
+    if fp32 and K >= 16:
+        assert any(var in (401, 402) for _, var in ran) and any(var in (501, 502) for _, var in ran)
     assert len(ran) >= 8
