@@ -1868,9 +1868,17 @@ int emg_spmm_layout_dev(emg_context *c, int fp32, int K, int v, int variant, con
     cvt_d2f(c->nnz, c->Cv.p, vc.p, s);
     cvt_d2f(c->nnz, c->Msv.p, vm.p, s);
     pack_records(c->nnz, c->ci.p, vc.p, vm.p, pk.p, s);
+    std::vector<int> crp;
+    const long nch = chunk_row_pointer(c->h_rp, crp);
+    DBuf<int> dcrp;
+    dcrp.upload(crp, s);
+    DBuf<int4> ch((size_t)std::max(3 * nch, 3L));
+    chunk_records(c->ne, c->rp.p, c->ci.p, vc.p, vm.p, dcrp.p, ch.p, s);
     a.vc = vc.p;
     a.vm = vm.p;
     a.pk = pk.p;
+    a.ch = ch.p;
+    a.crp = dcrp.p;
     ok = spmm_layout<float>(K, v, variant, a, s);
     EMG_CUDA(cudaStreamSynchronize(s));  // the temporaries are freed next
   } else {

@@ -79,6 +79,24 @@ SpmmFn spmm_pipe_pick() {
   else return nullptr;
 }
 
+// chunked kernel (spmm_chunk_kernel): nl = 601 (one block per SM minimum),
+// 604 (register-capped, 4 blocks per SM); FP32 two-part operators with the
+// chunked layout only
+template <typename T, int K, int V, int MINB>
+void spmm_chunk_launch(const SpmmArgs &a, cudaStream_t s) {
+  constexpr int RPW = 32 / (K / V);
+  long warps = ((long)a.n + RPW - 1) / RPW;
+  unsigned grid = (unsigned)((warps * 32 + 255) / 256);
+  if (grid == 0) return;
+  spmm_chunk_kernel<K, V, MINB><<<grid, 256, 0, s>>>(a);
+}
+
+template <typename T, int K, int V, int MINB>
+SpmmFn spmm_chunk_pick() {
+  if constexpr (spmm_legal<T, K, V, 1>() && sizeof(T) == 4 && K >= 8) return &spmm_chunk_launch<T, K, V, MINB>;
+  else return nullptr;
+}
+
 // packed-record variant (nl = 100 + NL): FP32 two-part operators only
 template <typename T, int K, int V, int NL>
 SpmmFn spmm_pick_packed() {
@@ -99,6 +117,8 @@ SpmmFn spmm_pick_nl(int nl) {
   case 101: return spmm_pick_packed<T, K, V, 1>();
   case 102: return spmm_pick_packed<T, K, V, 2>();
   case 104: return spmm_pick_packed<T, K, V, 4>();
+  case 601: return spmm_chunk_pick<T, K, V, 1>();
+  case 604: return spmm_chunk_pick<T, K, V, 4>();
   case 401: return spmm_pick_capped<T, K, V, 1, true>();
   case 402: return spmm_pick_capped<T, K, V, 2, true>();
   case 501: return spmm_pick_capped<T, K, V, 1, false>();
@@ -148,10 +168,12 @@ std::string SpmmTuner::report() const {
   std::ostringstream os;
   for (auto &kv : best)
     os << "T" << std::get<0>(kv.first) * 8 << " K" << std::get<1>(kv.first) << " nnz/row class "
-       << std::get<2>(kv.first) << " rows class " << (std::get<3>(kv.first) >> 1) << ": V=" << kv.second.first
+       << std::get<2>(kv.first) << " rows class " << (std::get<3>(kv.first) >> 2) << ": V=" << kv.second.first
        << (std::get<3>(kv.first) & 1 ? " (packed records available)" : "")
+       << (std::get<3>(kv.first) & 2 ? " (chunks available)" : "")
        << (kv.second.second < 0 ? " rows kernel B="
-                                : (kv.second.second > 500   ? " register-capped NL="
+                                : (kv.second.second > 600   ? " chunked, min blocks/SM "
+                                   : kv.second.second > 500 ? " register-capped NL="
                                    : kv.second.second > 400 ? " packed register-capped NL="
                                    : kv.second.second > 300 ? " packed pipelined U="
                                    : kv.second.second > 200 ? " pipelined U="
@@ -187,7 +209,8 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
   SpmmTuner &tn = tuner();
   int bucket = row_bucket(a, nnz);
   const bool packed = a.pk != nullptr && sizeof(T) == 4 && a.vm != nullptr;
-  auto key = std::make_tuple((int)sizeof(T), K, bucket, 2 * size_class(a) + (packed ? 1 : 0));
+  const bool chunked = a.ch != nullptr && a.crp != nullptr && sizeof(T) == 4 && a.vm != nullptr;
+  auto key = std::make_tuple((int)sizeof(T), K, bucket, 4 * size_class(a) + (packed ? 1 : 0) + (chunked ? 2 : 0));
   auto it = tn.best.find(key);
   std::pair<int, int> cfg;
   if (it != tn.best.end()) {
@@ -208,8 +231,9 @@ void spmm_nnz(int K, const SpmmArgs &a, long nnz, cudaStream_t s) {
       // then ran 17% slower over the solver's mix of smoothing modes.
       std::vector<std::pair<int, int>> cand;
       for (int v : {1, 2, 4})
-        for (int nl : {1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104, 401, 402, 501, 502}) {
+        for (int nl : {1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104, 401, 402, 501, 502, 601, 604}) {
           if (((nl > 100 && nl < 200) || (nl > 400 && nl < 500)) && !packed) continue;
+          if (nl > 600 && !chunked) continue;
           if (spmm_fn<T>(K, v, nl)) cand.push_back({v, nl});
         }
       // two interleaved passes, each candidate's best: one slow sample (a
@@ -305,6 +329,7 @@ bool spmm_layout(int K, int v, int nl, const SpmmArgs &a, cudaStream_t s) {
   if (!f) return false;
   const bool packed_variant = (nl > 100 && nl < 200) || (nl > 300 && nl < 400) || (nl > 400 && nl < 500);
   if (packed_variant && (a.pk == nullptr || a.vm == nullptr)) return false;
+  if (nl > 600 && (a.ch == nullptr || a.crp == nullptr || a.vm == nullptr)) return false;
   if (a.n > 0) f(a, s);
   EMG_LAUNCH_CHECK();
   return true;
@@ -316,6 +341,38 @@ __global__ void pack_records_kernel(long nnz, const int *__restrict__ ci, const 
                                     const float *__restrict__ vm, int4 *__restrict__ out) {
   const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (k < nnz) out[k] = make_int4(ci[k], __float_as_int(vc[k]), __float_as_int(vm[k]), 0);
+}
+
+// thread per row: the row's nonzeros into whole chunks of 4 (spmm_chunk_kernel)
+__global__ void chunk_records_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                     const float *__restrict__ vc, const float *__restrict__ vm,
+                                     const int *__restrict__ crp, int4 *__restrict__ ch) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int k0 = rp[r], k1 = rp[r + 1], q0 = crp[r], q1 = crp[r + 1];
+  int *out = reinterpret_cast<int *>(ch);
+  for (int t = 0; t < 4 * (q1 - q0); ++t) {
+    const int k = k0 + t;
+    const bool ok = k < k1;
+    const long base = 12L * (q0 + t / 4) + (t & 3);
+    out[base] = ok ? ci[k] : r;
+    out[base + 4] = ok ? __float_as_int(vc[k]) : 0;
+    out[base + 8] = ok ? __float_as_int(vm[k]) : 0;
+  }
+}
+
+long chunk_row_pointer(const std::vector<int> &rp, std::vector<int> &crp) {
+  const int n = (int)rp.size() - 1;
+  crp.assign(n + 1, 0);
+  for (int r = 0; r < n; ++r) crp[r + 1] = crp[r] + (rp[r + 1] - rp[r] + 3) / 4;
+  return n >= 0 ? crp[n] : 0;
+}
+
+void chunk_records(int n, const int *rp, const int *ci, const float *vc, const float *vm, const int *crp, int4 *ch,
+                   cudaStream_t s) {
+  if (n <= 0) return;
+  chunk_records_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, rp, ci, vc, vm, crp, ch);
+  EMG_LAUNCH_CHECK();
 }
 
 void pack_records(long nnz, const int *ci, const float *vc, const float *vm, int4 *out, cudaStream_t s) {

@@ -93,6 +93,11 @@ struct SpmmArgs {
   // FP32 two-part operators may also come as one 16-byte record per nonzero
   // (column, vc bits, vm bits, 0): one load per nonzero instead of three
   const int4 *pk;
+  // ... or in chunks of 4 nonzeros, rows padded to whole chunks: chunk q is
+  // three int4 at ch[3q]: columns, vc bits, vm bits (padding: column = the
+  // row, values 0); row r owns chunks crp[r] .. crp[r+1]
+  const int *crp;
+  const int4 *ch;
 };
 
 // One step of a fused nodal V-cycle (vcycle_fused_kernel): the operations a
@@ -376,6 +381,69 @@ __global__ void __launch_bounds__(256) spmm_pipe_kernel(SpmmArgs a) {
       for (int i = 0; i < V; ++i) acc[i] = fma(two ? cc[u] + w[i] * mm[u] : cc[u], xv[u][i], acc[i]);
   }
   epi_store<T, K, V>(a, row, cb, acc, w, two, epi);
+}
+
+// Chunked SpMM for FP32 two-part operators (SpmmArgs::ch): CL = K / V lanes
+// per row as spmm_kernel with NL = 1, but a row's nonzeros come in whole
+// chunks of 4 (three 16-byte loads per chunk, no bounds predicates, no zero
+// fills), and where the lane's V columns come in pairs with one frequency
+// (the real and imaginary parts of a complex column) each pair shares one
+// coefficient c + w m.
+template <bool PAIRS, int K, int V>
+__device__ __forceinline__ void chunk_rows(const SpmmArgs &a, int q0, int q1, int cb, const float (&w)[V],
+                                           float (&acc)[V]) {
+  const float *__restrict__ xb = static_cast<const float *>(a.x) + cb * V;
+  for (int q = q0; q < q1; ++q) {
+    const int4 jj = __ldg(a.ch + 3 * q);
+    const int4 cr = __ldg(a.ch + 3 * q + 1);
+    const int4 mr = __ldg(a.ch + 3 * q + 2);
+    const int j[4] = {jj.x, jj.y, jj.z, jj.w};
+    const float c[4] = {__int_as_float(cr.x), __int_as_float(cr.y), __int_as_float(cr.z), __int_as_float(cr.w)};
+    const float m[4] = {__int_as_float(mr.x), __int_as_float(mr.y), __int_as_float(mr.z), __int_as_float(mr.w)};
+    float xv[4][V];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) ldv<float, V>(xb + (long)j[u] * K, xv[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if constexpr (PAIRS) {
+#pragma unroll
+        for (int i = 0; i < V; i += 2) {
+          const float co = fmaf(w[i], m[u], c[u]);
+          acc[i] = fmaf(co, xv[u][i], acc[i]);
+          acc[i + 1] = fmaf(co, xv[u][i + 1], acc[i + 1]);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < V; ++i) acc[i] = fmaf(fmaf(w[i], m[u], c[u]), xv[u][i], acc[i]);
+      }
+    }
+  }
+}
+
+template <int K, int V, int MINB>
+__global__ void __launch_bounds__(256, MINB) spmm_chunk_kernel(SpmmArgs a) {
+  constexpr int CL = K / V;
+  static_assert(CL <= 32 && (32 % CL) == 0, "bad lane layout");
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int row = gwarp * (32 / CL) + lane / CL;
+  const int cb = lane % CL;
+  if (row >= a.n) return;  // no shuffles: a lane past the end leaves at once
+  float w[V], acc[V];
+  bool pairs = (V % 2) == 0;
+#pragma unroll
+  for (int i = 0; i < V; ++i) {
+    w[i] = (float)__ldg(a.omega + cb * V + i);
+    acc[i] = 0.f;
+  }
+#pragma unroll
+  for (int i = 0; i + 1 < V; i += 2) pairs = pairs && w[i] == w[i + 1];
+  EpiIn<float, V> epi;
+  epi_load<float, K, V>(a, row, cb, true, epi);
+  const int q0 = __ldg(a.crp + row), q1 = __ldg(a.crp + row + 1);
+  if (pairs) chunk_rows<true, K, V>(a, q0, q1, cb, w, acc);
+  else chunk_rows<false, K, V>(a, q0, q1, cb, w, acc);
+  epi_store<float, K, V>(a, row, cb, acc, w, true, epi);
 }
 
 // Row-group SpMM: G = K / V lanes serve one row (lane j owns column block j),

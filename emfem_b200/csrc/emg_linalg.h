@@ -43,6 +43,12 @@ template <typename T>
 bool spmm_layout(int K, int v, int nl, const SpmmArgs &a, cudaStream_t s);
 // FP32 two-part operator as one 16-byte record per nonzero (column, vc, vm, 0)
 void pack_records(long nnz, const int *ci, const float *vc, const float *vm, int4 *out, cudaStream_t s);
+// the same in chunks of 4 nonzeros per row (SpmmArgs::ch, spmm_chunk_kernel):
+// chunk row pointer from a host CSR row pointer (returns the chunk count),
+// then the chunks (3 int4 each) on the device
+long chunk_row_pointer(const std::vector<int> &rp, std::vector<int> &crp);
+void chunk_records(int n, const int *rp, const int *ci, const float *vc, const float *vm, const int *crp, int4 *ch,
+                   cudaStream_t s);
 
 // Tiles rows of a host CSR pattern for spmm_tiled: the largest R (a power of
 // two <= r_max, >= 8) whose busiest tile has at most umax_limit distinct

@@ -246,8 +246,17 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   if (sizeof(T) == 4 && !per_frequency) {
     ams.Bpk.alloc(c.nnz);
     pack_records(c.nnz, c.ci.p, (const float *)ams.B.vc.p, (const float *)ams.B.vm.p, ams.Bpk.p, s);
+    std::vector<int> crp;
+    const long nch = chunk_row_pointer(c.h_rp, crp);
+    ams.Bcrp.upload(crp, s);
+    ams.Bch.alloc((size_t)std::max(3 * nch, 3L));
+    chunk_records(c.ne, c.rp.p, c.ci.p, (const float *)ams.B.vc.p, (const float *)ams.B.vm.p, ams.Bcrp.p,
+                  ams.Bch.p, s);
+    EMG_CUDA(cudaStreamSynchronize(s));  // the host row pointer goes out of scope
   } else {
     ams.Bpk.release();
+    ams.Bch.release();
+    ams.Bcrp.release();
   }
   // edge tangents x(v1) - x(v0)
   {
@@ -487,6 +496,8 @@ void Ams<T>::spmm_B(int mode, const T *x, const T *b, T *y, cudaStream_t s) {
   SpmmArgs a;
   std::memset(&a, 0, sizeof(a));
   a.pk = Bpk.p;
+  a.ch = Bch.p;
+  a.crp = Bcrp.p;
   a.n = ne;
   a.rp = brp;
   a.ci = bci;
@@ -640,6 +651,8 @@ T *Ams<T>::smooth(const DCsr<T> *A, long nnz, int n, T *cur, T *oth, const T *b,
     SpmmArgs a;
     std::memset(&a, 0, sizeof(a));
     a.pk = edge ? Bpk.p : nullptr;
+    a.ch = edge ? Bch.p : nullptr;
+    a.crp = edge ? Bcrp.p : nullptr;
     a.n = n;
     a.rp = edge ? brp : A->rp.p;
     a.ci = edge ? bci : A->ci.p;

@@ -104,6 +104,8 @@ struct Ams {
   Context *ctx = nullptr;          // owner of the fixed patterns (tiled copies)
   DCsr<T> B;                       // values only: pattern is the context's
   DBuf<int4> Bpk;                  // FP32 two-part B as packed records (column, vc, vm, 0); empty otherwise
+  DBuf<int4> Bch;                  // the same in chunks of 4 nonzeros per row (SpmmArgs::ch); empty otherwise
+  DBuf<int> Bcrp;                  // chunk row pointer of Bch
   const int *brp = nullptr, *bci = nullptr;
   long nnzB = 0;
   bool two = true;  // two value parts (batched) or combined (one frequency)

@@ -391,8 +391,10 @@ int emg_spmv_complex_dev(emg_context *ctx, int k, const double *omegas_host, con
  * 100 + NL / 300 + U packed 16-byte records (fp32 only), 200 + U the
  * software-pipelined kernel with chunks of U nonzeros, 400 + NL / 500 + NL
  * the row-split kernel capped at 64 registers (4 blocks per SM; packed
- * records / arrays, fp32, K >= 16).  EMG_ERR_ARG for a layout not built for
- * K.  Tests every kernel the autotuner can pick. */
+ * records / arrays, fp32, K >= 16), 601 / 604 the chunked kernel (rows in
+ * whole chunks of 4 nonzeros; fp32, K >= 8; 604 register-capped).
+ * EMG_ERR_ARG for a layout not built for K.  Tests every kernel the
+ * autotuner can pick. */
 int emg_spmm_layout_dev(emg_context *ctx, int fp32, int K, int v, int variant, const double *omegas_host,
                         const void *x_dev, const void *b_dev, void *y_dev);
 /* the nodal AMG hierarchy of AMS subspace sp (0 gradient, 1-3 Pi_x/y/z, 4 the

@@ -1,7 +1,8 @@
 """Every SpMM lane layout the autotuner can pick, against a float64 product.
 
 The block solver times all legal layouts of its SpMM (row-split, row-group,
-packed-record and software-pipelined kernels, 1/2/4 columns per vector load)
+packed-record, software-pipelined, register-capped and chunked kernels, 1/2/4
+columns per vector load)
 on the first large operator it meets and keeps the fastest; the test meshes
 are too small to trigger that tuning, so this test forces each layout through
 emg_spmm_layout_dev on the assembled edge operator B = C + w_c Ms and checks
@@ -20,7 +21,7 @@ import emfem_b200 as E
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104, 204, 208, 304, 308, 401, 402, 501, 502]
+VARIANTS = [1, 2, 4, 8, 16, 32, -4, -8, 101, 102, 104, 204, 208, 304, 308, 401, 402, 501, 502, 601, 604]
 
 
 @pytest.fixture(scope="module")
@@ -80,4 +81,6 @@ def test_every_layout_matches_float64(edge_operator, fp32, K):
         assert any(var in (304, 308) for _, var in ran)
     if fp32 and K >= 16:
         assert any(var in (401, 402) for _, var in ran) and any(var in (501, 502) for _, var in ran)
+    if fp32:
+        assert any(var in (601, 604) for _, var in ran)
     assert len(ran) >= 8
