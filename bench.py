@@ -305,11 +305,11 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
     t_step = float(np.mean(times))
     # A/B on the target columns: zero start and the interpolation alone
     ab = {}
-    for arm in ("zero", "interp"):
+    for arm in ("zero", "interp", "network"):
         xt.zero_()
-        if arm == "interp":
+        if arm != "zero":
             ctx.warm_start_predict(fa, fsa, xa.data_ptr(), ft, fst, xt.data_ptr(), src_pos=pos_a, tsrc_pos=pos_t,
-                                   network=False)
+                                   network=(arm == "network"))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         inf = ctx.solve_block_dev(ft, st.data_ptr(), xt.data_ptr(), rtol=1e-8, max_it=200, inner_fp32=True,
@@ -348,11 +348,15 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
         "target_block_ms_zero": ab["zero"]["block_ms"],
         "target_outer_its_interp": ab["interp"]["outer_its"], "target_inner_its_interp": ab["interp"]["inner_its"],
         "target_initial_res_interp": ab["interp"]["initial_res"], "target_block_ms_interp": ab["interp"]["block_ms"],
+        "target_outer_its_network_forced": ab["network"]["outer_its"],
+        "target_inner_its_network_forced": ab["network"]["inner_its"],
+        "target_initial_res_network_forced": ab["network"]["initial_res"],
+        "target_block_ms_network_forced": ab["network"]["block_ms"],
         "single_block_solve_ms": single_ms,
     }
-    log("warm start: %.1f ms/step; target its network %s zero %s interp %s" % (
+    log("warm start: %.1f ms/step; target its guess %s zero %s interp %s network %s" % (
         out["ms_per_step"], out["target_outer_its_network"], out["target_outer_its_zero"],
-        out["target_outer_its_interp"]))
+        out["target_outer_its_interp"], out["target_outer_its_network_forced"]))
     return out
 
 
