@@ -253,6 +253,7 @@ static void parse_options(Options &o, const std::string &text, std::vector<std::
     else if (key == "emg_amg_cheb_degree") o.amg_cheb_degree = geti(k, v);
     else if (key == "emg_restrict_smooth") o.restrict_j0 = v.empty() ? 1 : getb(v);
     else if (key == "emg_block_floor_stop") o.block_floor_stop = v.empty() ? 1 : getb(v);
+    else if (key == "emg_amg_pre_smooth") o.amg_pre_smooth = v.empty() ? 1 : getb(v);
     else if (key == "emg_spmm_tiled") o.spmm_tiled = v.empty() ? 1 : getb(v);
     else if (key == "emg_tiled_smem_kb") o.tiled_smem_kb = geti(k, v);
     else if (key == "emg_verbose") o.verbose = v.empty() ? 1 : geti(k, v);
@@ -683,6 +684,7 @@ int emg_get_option(emg_context *ctx, const char *key, double *value) {
   else if (k == "emg_amg_cheb_degree") *value = o.amg_cheb_degree;
   else if (k == "emg_restrict_smooth") *value = o.restrict_j0;
   else if (k == "emg_block_floor_stop") *value = o.block_floor_stop;
+  else if (k == "emg_amg_pre_smooth") *value = o.amg_pre_smooth;
   else if (k == "emg_spmm_tiled") *value = o.spmm_tiled;
   else if (k == "emg_tiled_smem_kb") *value = o.tiled_smem_kb;
   else fail(EMG_ERR_OPTION, "unknown option %s", key);

@@ -176,6 +176,7 @@ struct Options {
   int block_cheb_degree = 4;
   int amg_cheb_degree = 2;    // the same on the nodal AMG levels
   int restrict_j0 = 1;        // nodal restrictions take the fed level's first smoothing step
+  int amg_pre_smooth = 1;     // nodal levels smooth before the coarse correction (V(m, m)) or not (V(0, m))
   int block_floor_stop = 1;   // block FGMRES columns stop at the rounding floor of their residual
   int gpu_amg = 1;        // nodal AMG setup on the device (1) or on the host (0)
   int block_fp64_fallback = 1;  // batched path: columns the FP32 AMS leaves unconverged finish in FP64

@@ -33,10 +33,12 @@ void spmm_launch(const SpmmArgs &a, cudaStream_t s) {
 }
 
 // register-capped row-split kernel (nl = 400 + NL packed records, 500 + NL
-// index and value arrays): 4 blocks of 256 threads per SM; FP32, K >= 16
+// index and value arrays): 4 blocks of 256 threads per SM; K >= 16 (packed
+// records: FP32 only)
 template <typename T, int K, int V, int NL, bool PK>
 SpmmFn spmm_pick_capped() {
-  if constexpr (spmm_legal<T, K, V, NL>() && sizeof(T) == 4 && K >= 16) return &spmm_launch<T, K, V, NL, PK, 4>;
+  if constexpr (spmm_legal<T, K, V, NL>() && (sizeof(T) == 4 || !PK) && K >= 16)
+    return &spmm_launch<T, K, V, NL, PK, 4>;
   else return nullptr;
 }
 

@@ -198,6 +198,7 @@ void ams_setup(Context &c, Ams<T> &ams, bool per_frequency, double w, double w_r
   ams.cheb_degree = per_frequency ? c.opt.cheb_degree : c.opt.block_cheb_degree;
   ams.amg_cheb_degree = c.opt.amg_cheb_degree;
   ams.restrict_j0 = c.opt.restrict_j0 != 0;
+  ams.amg_pre_smooth = c.opt.amg_pre_smooth != 0;
   ams.two = !per_frequency;
   ams.use_graphs = c.opt.graphs != 0;
   ams.fused = c.opt.ams_fused != 0;
@@ -721,13 +722,26 @@ void Ams<T>::vcycle(int sp, int l, cudaStream_t s, bool started) {
   const int n = lv.A.n;
   const char *bin = sizeof(T) == 4 ? "spmm_nodal_fp32" : "spmm_nodal_fp64";
   // out-of-place smoothing applications after the zero-guess one:
-  // (amg_relax_times - 1) pre + amg_relax_times post; start in the buffer
-  // that makes the last one land in wx
-  const int swaps = 2 * amg_relax_times - 1;
+  // (amg_relax_times - 1) pre + amg_relax_times post (without pre-smoothing:
+  // the amg_relax_times post ones); start in the buffer that makes the last
+  // one land in wx
+  const int swaps = amg_pre_smooth ? 2 * amg_relax_times - 1 : amg_relax_times;
   T *cur = (swaps & 1) ? wx2[sp][l].p : wx[sp][l].p;
   T *oth = (swaps & 1) ? wx[sp][l].p : wx2[sp][l].p;
   const T *b = wb[sp][l].p;
   T *r = wr[sp][l].p, *d = wd[sp][l].p, *d2 = wd2[sp][l].p;
+  if (!amg_pre_smooth) {
+    // V(0, m): zero start, so the residual is b itself; the coarse
+    // correction P e is the first iterate
+    emit_spmm(level_args<T>(lv.R, SPMM_AX, nullptr, 1.0, b, nullptr, wb[sp][l + 1].p), lv.nnzR, bin, s);
+    vcycle(sp, l + 1, s, false);
+    emit_spmm(level_args<T>(lv.P, SPMM_AX, nullptr, 1.0, wx[sp][l + 1].p, nullptr, cur), lv.nnzP, bin, s);
+    for (int it = 0; it < amg_relax_times; ++it) {
+      T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, d2, false, bin, s);
+      if (res != cur) std::swap(cur, oth);
+    }
+    return;
+  }
   for (int it = 0; it < amg_relax_times; ++it) {
     T *res = smooth(&lv.A, lv.nnzA, n, cur, oth, b, r, d, d2, it == 0, bin, s, started && it == 0);
     if (res != cur) std::swap(cur, oth);

@@ -126,6 +126,7 @@ struct Ams {
   int cheb_degree = 2;             // operator applications per edge smoothing sweep
   int amg_cheb_degree = 2;         // the same on the nodal levels
   bool restrict_j0 = true;         // restrictions take the fed level's first smoothing step
+  bool amg_pre_smooth = true;      // nodal V(m, m) cycles; false: V(0, m)
   bool use_graphs = true;          // replay each application as one CUDA graph
   bool split_gradient = false;     // last '1' of the cycle returned as potential gphi()
   // each nodal V-cycle as one cooperative launch (emg_fused.cu) instead of

@@ -29,7 +29,8 @@ staged once in shared memory), with the default 64 KB and with small tiles
 recurrence's middle steps) on the edges of both solvers and on the nodal
 levels, stepwise and in the fused V-cycle; and with each nodal restriction
 taking the fed level's first smoothing step (the default) or leaving it to
-its own launch, for Chebyshev and l1-Jacobi smoothing.
+its own launch, for Chebyshev and l1-Jacobi smoothing; and with nodal V(0, m)
+cycles (no pre-smoothing), stepwise and fused.
 """
 
 import numpy as np
@@ -105,7 +106,9 @@ def _direct(rp, ci, Cv, Mv, sr, si):
                                    "-emg_fused_rows 400",
                                    "-emg_restrict_smooth 0",
                                    "-emg_restrict_smooth 0 -emg_smoother l1jacobi",
-                                   "-emg_smoother l1jacobi"])
+                                   "-emg_smoother l1jacobi",
+                                   "-emg_amg_pre_smooth 0",
+                                   "-emg_amg_pre_smooth 0 -emg_amg_relax_times 2 -emg_fused_vcycle 1 -emg_fused_rows 400"])
 def test_pi_vector_space_cycles(mt_small, extra):
     prob = mt_small
     bg = mg.background_model(prob.mesh, prob.model)
