@@ -305,11 +305,11 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
     t_step = float(np.mean(times))
     # A/B on the target columns: zero start and the interpolation alone
     ab = {}
-    for arm in ("zero", "interp", "network"):
+    for arm in ("zero", "interp", "network", "quadratic"):
         xt.zero_()
         if arm != "zero":
             ctx.warm_start_predict(fa, fsa, xa.data_ptr(), ft, fst, xt.data_ptr(), src_pos=pos_a, tsrc_pos=pos_t,
-                                   network=(arm == "network"))
+                                   network={"interp": 0, "network": 1, "quadratic": 3}[arm])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         inf = ctx.solve_block_dev(ft, st.data_ptr(), xt.data_ptr(), rtol=1e-8, max_it=200, inner_fp32=True,
@@ -352,11 +352,14 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
         "target_inner_its_network_forced": ab["network"]["inner_its"],
         "target_initial_res_network_forced": ab["network"]["initial_res"],
         "target_block_ms_network_forced": ab["network"]["block_ms"],
+        "target_outer_its_quadratic": ab["quadratic"]["outer_its"],
+        "target_initial_res_quadratic": ab["quadratic"]["initial_res"],
+        "target_block_ms_quadratic": ab["quadratic"]["block_ms"],
         "single_block_solve_ms": single_ms,
     }
-    log("warm start: %.1f ms/step; target its guess %s zero %s interp %s network %s" % (
+    log("warm start: %.1f ms/step; target its guess %s zero %s interp %s network %s quadratic %s" % (
         out["ms_per_step"], out["target_outer_its_network"], out["target_outer_its_zero"],
-        out["target_outer_its_interp"], out["target_outer_its_network_forced"]))
+        out["target_outer_its_interp"], out["target_outer_its_network_forced"], out["target_outer_its_quadratic"]))
     return out
 
 
@@ -698,7 +701,13 @@ def ours(args):
                         "workload (launch by launch) right after the timed region",
             "share_of_profiled_step": t_l / (prof_step_s * 1e3) if prof_step_s > 0 else None,
             "other_bins_share_of_profiled_step": {b: round(bins[b][1] / (prof_step_s * 1e3), 4)
-                                                  for b in bins if b != dom and bins[b][0] and prof_step_s > 0}}
+                                                  for b in bins if b != dom and bins[b][0] and prof_step_s > 0},
+            # the other SpMM families beside the roofline kernel: algorithmic GB/s over their summed
+            # launch times (the nodal bin spans many small, mostly L2-resident launch shapes)
+            "other_bins": {b: {"launches": bins[b][0], "avg_launch_us": round(1e3 * bins[b][1] / bins[b][0], 2),
+                               "achieved_gbs": round(bins[b][2] / (bins[b][1] * 1e-3) / 1e9, 1),
+                               "frac": round(bins[b][2] / (bins[b][1] * 1e-3) / 1e9 / peak, 4)}
+                           for b in bins if b != dom and bins[b][0] and bins[b][1] > 0}}
 
     # ---- e2e through the host-buffer C ABI ----------------------------------
     e2e = None

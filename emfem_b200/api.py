@@ -599,7 +599,7 @@ class EMContext:
         _check(lib().emg_warm_start_predict(self._h, f.size, _ptr(f), _ptr(s), None if p is None else _ptr(p),
                                             C.c_void_p(x_ptr), tf.size, _ptr(tf), _ptr(ts),
                                             None if tp is None else _ptr(tp),
-                                            network if network in (0, 1, 2) else int(bool(network)),
+                                            network if network in (0, 1, 2, 3) else int(bool(network)),
                                             C.c_void_p(guess_ptr)))
 
     def warm_start_params(self, set_to=None):

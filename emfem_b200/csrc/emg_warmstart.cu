@@ -61,6 +61,53 @@ bool neighbours(const std::vector<Column> &solved, const Column &t, int skip, Sp
   return true;
 }
 
+// three-point Lagrange interpolation in log f: the three solved columns of
+// the same source nearest to the target, used only when the target lies
+// inside their frequency range (no extrapolation); false otherwise
+struct Quad {
+  int tcol, c[3];
+  double w[3];
+};
+
+bool quad_neighbours(const std::vector<Column> &solved, const Column &t, Quad &q) {
+  std::vector<std::pair<double, int>> cand;
+  for (int j = 0; j < (int)solved.size(); ++j)
+    if (solved[j].src == t.src) cand.push_back({std::fabs(std::log(solved[j].f / t.f)), j});
+  if (cand.size() < 3) return false;
+  std::sort(cand.begin(), cand.end());
+  double u[3], lo = 1e300, hi = -1e300;
+  for (int i = 0; i < 3; ++i) {
+    q.c[i] = cand[i].second;
+    u[i] = std::log(solved[q.c[i]].f);
+    lo = std::min(lo, u[i]);
+    hi = std::max(hi, u[i]);
+  }
+  const double ut = std::log(t.f);
+  if (u[0] == u[1] || u[0] == u[2] || u[1] == u[2] || ut < lo || ut > hi) return false;
+  for (int i = 0; i < 3; ++i) {
+    const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+    q.w[i] = (ut - u[i1]) * (ut - u[i2]) / ((u[i] - u[i1]) * (u[i] - u[i2]));
+  }
+  return true;
+}
+
+// out[:, tcol] = sum_i w_i xs[:, c_i] for every target (complex columns)
+__global__ void lagrange3_kernel(long ne, int ks, int kt, int nq, const Quad *__restrict__ q,
+                                 const double2 *__restrict__ xs, double2 *__restrict__ out) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= ne * nq) return;
+  const long e = t / nq;
+  const Quad qq = q[t - e * nq];
+  double2 v = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double2 x = xs[e * ks + qq.c[i]];
+    v.x += qq.w[i] * x.x;
+    v.y += qq.w[i] * x.y;
+  }
+  out[e * kt + qq.tcol] = v;
+}
+
 std::vector<Spec> training_specs(const std::vector<Column> &cols) {
   std::vector<Spec> specs;
   for (int j = 0; j < (int)cols.size(); ++j) {
@@ -137,12 +184,35 @@ int emg_warm_start_predict(emg_context *c, int k, const double *freqs, const int
     sp.tcol = j;
     specs.push_back(sp);
   }
-  need(network >= 0 && network <= 2, EMG_ERR_ARG, "network must be 0, 1 or 2");
+  need(network >= 0 && network <= 3, EMG_ERR_ARG, "network must be 0, 1, 2 or 3");
   // 2: the network only where training showed it halves the interpolation's
   // curvature error (a quarter of its squared loss on the same samples)
   const bool use_net = network == 1 || (network == 2 && net.last_loss >= 0 && net.last_loss0 > 0 &&
                                         net.last_loss <= 0.25 * net.last_loss0);
-  if (!specs.empty()) net.predict(*c, x_dev, k, specs, guess_dev, kt, use_net);
+  if (network == 3) {
+    // quadratic in log f where three solved columns bracket the target; the
+    // linear interpolation for the rest
+    std::vector<Quad> quads;
+    std::vector<Spec> lin;
+    for (const Spec &sp : specs) {
+      Quad q;
+      q.tcol = sp.tcol;
+      if (quad_neighbours(cols, tg[sp.tcol], q)) quads.push_back(q);
+      else lin.push_back(sp);
+    }
+    if (!lin.empty()) net.predict(*c, x_dev, k, lin, guess_dev, kt, false);
+    if (!quads.empty()) {
+      DBuf<Quad> qd;
+      qd.upload(quads, c->stream);
+      const long total = (long)c->ne * (long)quads.size();
+      lagrange3_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
+          c->ne, k, kt, (int)quads.size(), qd.p, (const double2 *)x_dev, (double2 *)guess_dev);
+      EMG_LAUNCH_CHECK();
+      EMG_CUDA(cudaStreamSynchronize(c->stream));  // qd is freed next
+    }
+  } else if (!specs.empty()) {
+    net.predict(*c, x_dev, k, specs, guess_dev, kt, use_net);
+  }
   EMG_CUDA(cudaStreamSynchronize(c->stream));
   net.check(c->stream);
   EMG_API_END

@@ -103,6 +103,37 @@ def test_predictions_match_cpu(small):
             assert np.abs(g[:, j] - ref).max() <= tol * np.abs(ref).max(), (network, j)
 
 
+def test_quadratic_guess_matches_lagrange(small):
+    """Mode 3: three-point Lagrange interpolation in log f where the three
+    nearest solved columns of the source bracket the target (0.3 Hz, 3 Hz:
+    bracketed by 0.1, 1, 10 Hz), the log-f interpolation elsewhere (0.05 Hz,
+    30 Hz); FP64 arithmetic, 1e-12."""
+    import torch
+    c = small["ctx"]
+    ne = small["prob"].mesh.n_edges
+    tf = np.array([0.3, 3.0, 0.05, 30.0])
+    ts = np.array([0, 1, 1, 0], dtype=np.int32)
+    gd = torch.zeros((ne, tf.size), dtype=torch.complex128, device="cuda")
+    c.warm_start_predict(small["freqs"], small["src"], small["xd"].data_ptr(), tf, ts, gd.data_ptr(), network=3)
+    g = gd.cpu().numpy()
+    lin = torch.zeros_like(gd)
+    c.warm_start_predict(small["freqs"], small["src"], small["xd"].data_ptr(), tf, ts, lin.data_ptr(), network=0)
+    lin = lin.cpu().numpy()
+    xs, freqs, src = small["xs"], small["freqs"], small["src"]
+    for j in range(2):
+        cols = [i for i in range(freqs.size) if src[i] == ts[j]]
+        u = np.log(freqs[cols])
+        ut = np.log(tf[j])
+        ref = np.zeros(ne, dtype=np.complex128)
+        for a in range(3):
+            w = np.prod([(ut - u[b]) / (u[a] - u[b]) for b in range(3) if b != a])
+            ref += w * xs[:, cols[a]]
+        assert np.abs(g[:, j] - ref).max() <= 1e-12 * np.abs(ref).max(), j
+        assert np.abs(g[:, j] - lin[:, j]).max() > 1e-6 * np.abs(ref).max()  # not the linear guess
+    for j in range(2, 4):  # outside the solved range: the linear interpolation
+        assert np.abs(g[:, j] - lin[:, j]).max() <= 1e-12 * np.abs(lin[:, j]).max(), j
+
+
 @pytest.fixture(scope="module")
 def ab_runs():
     """Anchors (every other frequency, both polarisations) solved from zero;
