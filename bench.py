@@ -327,7 +327,8 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
                     "forward and backward kernels, Adam"),
         "schedule": ("anchor columns (frequencies %s, every source) solved from zero; network trained on them "
                      "(%d Adam steps of %d samples); the other %d columns solved from its guess (the network's "
-                     "correction only where its training loss is a quarter of the interpolation's)"
+                     "correction where its training loss is a quarter of the interpolation's, else the quadratic "
+                     "log-f interpolation)"
                      % ([float(f) for f in cols.freqs[::2]], args.warm_steps, args.warm_batch, kt)),
         "value": cols.k / t_step, "unit": UNIT, "ms_per_step": 1e3 * t_step, "steps_timed": n_t,
         "timing": "host wall clock around the whole two-stage step (assembly, right-hand sides, both solves, "
@@ -336,7 +337,8 @@ def warm_start_arm(args, ctx, cols, rhs, ne, infos_single):
         "target_block_ms": 1e3 * rec["t_target"], "train_loss": rec["loss"],
         "train_loss_interpolation": rec["losses"][1],
         "guess": ("network" if 0 <= rec["losses"][0] <= 0.25 * rec["losses"][1] else
-                  "interpolation (the network's training loss was above a quarter of the interpolation's)"),
+                  "quadratic log-f interpolation where three anchors bracket the target, linear elsewhere (the "
+                  "network's training loss was above a quarter of the linear interpolation's)"),
         "anchor_outer_its": [i.outer_its for i in rec["inf_a"]],
         "anchor_inner_its": int(rec["inf_a"][0].inner_its),
         "target_outer_its_network": [i.outer_its for i in rec["inf_t"]],

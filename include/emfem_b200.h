@@ -359,11 +359,11 @@ int emg_warm_start_train(emg_context *ctx, int k, const double *freqs, const int
 /* guesses for kt target columns into guess_dev (n_edges x kt complex);
  * network 0: the log-f interpolation alone, 1: interpolation plus the
  * network's correction, 2: the network only if the last training step's loss
- * was at most a quarter of the interpolation's on the same samples, else the
- * interpolation; 3: three-point Lagrange interpolation in log f from the
- * three nearest solved columns of the source where they bracket the target,
- * the log-f interpolation elsewhere (no network); a target without a solved
- * column of its source gets zero */
+ * was at most a quarter of the interpolation's on the same samples, else as
+ * 3; 3: three-point Lagrange interpolation in log f from the three nearest
+ * solved columns of the source where they bracket the target, the log-f
+ * interpolation elsewhere (no network); a target without a solved column of
+ * its source gets zero */
 int emg_warm_start_predict(emg_context *ctx, int k, const double *freqs, const int *src, const double *src_pos,
                            const double *x_dev, int kt, const double *tfreqs, const int *tsrc,
                            const double *tsrc_pos, int network, double *guess_dev);

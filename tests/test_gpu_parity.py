@@ -7,7 +7,7 @@ Tolerances (written per test):
     order (atomics, closed-form instead of quadrature) -> 1e-12 relative to the
     largest entry of the array;
   * solves: true relative residual <= rtol in FP64, receiver fields within
-    1e-6 relative of the oracle's FP64 solve.
+    1e-6 relative of the oracle's FP64 solve (the receiver-field accuracy bar).
 """
 
 import numpy as np
