@@ -95,6 +95,7 @@ _SIGS = {
     "emg_solve_block_dev": ([_P, _I, _P, _P, _P, C.POINTER(BlockOpts), _P], _I),
     "emg_spmv_complex_dev": ([_P, _I, _P, _P, _P, _I], _I),
     "emg_spmm_layout_dev": ([_P, _I, _I, _I, _I, _P, _P, _P, _P], _I),
+    "emg_orient3d_sign": ([_P, _P, _P, _P, C.POINTER(_I)], _I),
     "emg_last_kernel_ms": ([_P, C.c_char_p, C.POINTER(_D)], _I),
     "emg_stream_synchronize": ([_P], _I),
     "emg_launch_count": ([C.POINTER(C.c_long)], _I),
@@ -171,6 +172,14 @@ def launch_count() -> int:
     n = C.c_long()
     _check(lib().emg_launch_count(C.byref(n)))
     return n.value
+
+
+def orient3d_sign(a, b, c, d) -> int:
+    """exact sign of det[a-d; b-d; c-d] (the point-location predicate)"""
+    pts = [_f64(np.asarray(v, dtype=np.float64).reshape(3)) for v in (a, b, c, d)]
+    out = _I()
+    _check(lib().emg_orient3d_sign(_ptr(pts[0]), _ptr(pts[1]), _ptr(pts[2]), _ptr(pts[3]), C.byref(out)))
+    return out.value
 
 
 def spmm_layouts() -> str:

@@ -227,4 +227,11 @@ int emg_calculate_response_csem(int nrx, const double *fields, int nobs, const i
   EMG_API_END
 }
 
+int emg_orient3d_sign(const double *a, const double *b, const double *c, const double *d, int *sign) {
+  EMG_API_BEGIN
+  need(a && b && c && d && sign, EMG_ERR_ARG, "null argument");
+  *sign = emg::orient3d_sign(a, b, c, d);
+  EMG_API_END
+}
+
 }  // extern "C"

@@ -8,8 +8,9 @@
 // closest vertex comes from a uniform grid of the vertices (exact nearest
 // neighbour, ties to the lowest vertex index) and the visited set is a
 // per-query hash set, so a query costs the walk it makes and nothing more.
-// The walk and the containment test are the reference's, so every point gets
-// the same tet, ties on shared faces included.
+// The walk and the containment test are the reference's, with the exact
+// orientation sign of its predicate, so every point gets the same tet, ties
+// on shared faces included.
 
 #include <algorithm>
 #include <cmath>
@@ -23,10 +24,74 @@ namespace emg {
 
 namespace {
 
-// orient3d(a,b,c,d) = det[a-d; b-d; c-d] with a floating-point filter and an
-// extended-precision re-evaluation near zero (the reference uses exact
-// predicates; this filter resolves every case but points within rounding of
-// a face plane, where either neighbouring tet is a valid answer).
+// Exact sign of a sum of products of doubles with floating-point expansions
+// (Shewchuk, "Adaptive precision floating-point arithmetic and fast robust
+// geometric predicates", Discrete Comput. Geom. 18, 1997): a value is an
+// unevaluated sum of doubles of increasing magnitude that do not overlap, so
+// its sign is the sign of its largest nonzero term.  Round to nearest; no
+// FMA contraction in the error-free transformations (fma is called only
+// where its single rounding is the point: the product's error term).
+struct Expansion {
+  double t[160];
+  int n = 0;
+  // e += b exactly (grow-expansion with zero elimination)
+  void add(double b) {
+    int m = 0;
+    double q = b;
+    for (int i = 0; i < n; ++i) {
+      const double x = q + t[i];
+      const double bv = x - q, av = x - bv;
+      const double err = (q - av) + (t[i] - bv);
+      q = x;
+      if (err != 0.0) t[m++] = err;
+    }
+    if (q != 0.0 || m == 0) t[m++] = q;
+    n = m;
+  }
+  // e += sign * p * q * r exactly: p q = hi + lo (two-product), then each
+  // part times r is again a two-product, four terms in all
+  void add_product3(double sign, double p, double q, double r) {
+    const double hi = p * q, lo = std::fma(p, q, -hi);
+    const double a = hi * r, ae = std::fma(hi, r, -a);
+    const double b = lo * r, be = std::fma(lo, r, -b);
+    add(sign * be);
+    add(sign * b);
+    add(sign * ae);
+    add(sign * a);
+  }
+  int sign() const {
+    for (int i = n - 1; i >= 0; --i)
+      if (t[i] != 0.0) return t[i] > 0.0 ? 1 : -1;
+    return 0;
+  }
+};
+
+// sign of det3 of rows p, q, r, added to e with the given sign
+void add_det3(Expansion &e, double sign, const double *p, const double *q, const double *r) {
+  e.add_product3(sign, p[0], q[1], r[2]);
+  e.add_product3(-sign, p[0], q[2], r[1]);
+  e.add_product3(-sign, p[1], q[0], r[2]);
+  e.add_product3(sign, p[1], q[2], r[0]);
+  e.add_product3(sign, p[2], q[0], r[1]);
+  e.add_product3(-sign, p[2], q[1], r[0]);
+}
+
+// exact sign of det[a-d; b-d; c-d] = det4 of the rows (x, y, z, 1) of a, b,
+// c, d = det3(a,b,c) - det3(a,b,d) + det3(a,c,d) - det3(b,c,d), evaluated on
+// the input coordinates themselves (the differences a - d would round)
+int orient3d_exact(const double *a, const double *b, const double *c, const double *d) {
+  Expansion e;
+  add_det3(e, 1.0, a, b, c);
+  add_det3(e, -1.0, a, b, d);
+  add_det3(e, 1.0, a, c, d);
+  add_det3(e, -1.0, b, c, d);
+  return e.sign();
+}
+
+// orient3d(a,b,c,d) = det[a-d; b-d; c-d] (TetGen's robust predicate, whose
+// sign is exact): a floating-point filter (error bound 1e-14 of the
+// permanent, above the 7.8e-16 that bounds the rounding of this evaluation),
+// then the exact sign from orient3d_exact
 double orient3d(const double *a, const double *b, const double *c, const double *d) {
   const double adx = a[0] - d[0], bdx = b[0] - d[0], cdx = c[0] - d[0];
   const double ady = a[1] - d[1], bdy = b[1] - d[1], cdy = c[1] - d[1];
@@ -36,15 +101,15 @@ double orient3d(const double *a, const double *b, const double *c, const double 
                       (std::fabs(cdy * adz) + std::fabs(cdz * ady)) * std::fabs(bdx) +
                       (std::fabs(ady * bdz) + std::fabs(adz * bdy)) * std::fabs(cdx);
   if (std::fabs(det) > 1e-14 * perm) return det;
-  typedef long double LD;
-  const LD Adx = (LD)a[0] - d[0], Bdx = (LD)b[0] - d[0], Cdx = (LD)c[0] - d[0];
-  const LD Ady = (LD)a[1] - d[1], Bdy = (LD)b[1] - d[1], Cdy = (LD)c[1] - d[1];
-  const LD Adz = (LD)a[2] - d[2], Bdz = (LD)b[2] - d[2], Cdz = (LD)c[2] - d[2];
-  const LD D = Adx * (Bdy * Cdz - Bdz * Cdy) + Bdx * (Cdy * Adz - Cdz * Ady) + Cdx * (Ady * Bdz - Adz * Bdy);
-  return (double)D;
+  return (double)orient3d_exact(a, b, c, d);
 }
 
 }  // namespace
+
+int orient3d_sign(const double *a, const double *b, const double *c, const double *d) {
+  const double v = orient3d(a, b, c, d);
+  return v > 0.0 ? 1 : (v < 0.0 ? -1 : 0);
+}
 
 PointIndex::PointIndex(int nv_, const double *pts_, int nt_, const int *tets_, const int *nbr_)
     : nv(nv_), nt(nt_), pts(pts_, pts_ + 3 * (size_t)nv_), tets(tets_, tets_ + 4 * (size_t)nt_),

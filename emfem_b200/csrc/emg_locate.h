@@ -6,6 +6,10 @@
 
 namespace emg {
 
+// sign (-1, 0, 1) of orient3d(a, b, c, d) = det[a-d; b-d; c-d], exact (the
+// sign of TetGen's robust predicate, which the containment test reads)
+int orient3d_sign(const double *a, const double *b, const double *c, const double *d);
+
 struct PointIndex {
   int nv = 0, nt = 0;
   std::vector<double> pts;

@@ -195,6 +195,10 @@ int emg_interpolate_fields_host(emg_context *ctx, int fidx, int n, const double 
 typedef struct emg_point_index emg_point_index;
 emg_point_index *emg_point_index_create(int nv, const double *pts, int nt, const int *tets, const int *nbr);
 int emg_point_index_find(const emg_point_index *idx, int n, const double *pts, int *tets_out);
+/* *sign = the exact sign (-1, 0, 1) of orient3d(a, b, c, d) = det[a-d; b-d;
+ * c-d] for 3-vectors a..d: the predicate behind TetAccessor::contains_point
+ * (src/em_mesh.h:208-230), whose robust orient3d has an exact sign */
+int emg_orient3d_sign(const double *a, const double *b, const double *c, const double *d, int *sign);
 void emg_point_index_destroy(emg_point_index *idx);
 /* the same on the context's mesh (index built on first use, dropped by the
  * next emg_set_mesh) */

@@ -169,8 +169,56 @@ struct Tet {
   }
 };
 
-// orient3d(a,b,c,d) = det[a-d; b-d; c-d]: floating-point filter with an
-// extended-precision re-evaluation near zero (TetGen uses exact predicates).
+// Exact sign of det[a-d; b-d; c-d]: TetGen's orient3d (a robust predicate
+// whose sign is exact; it is a third-party source absent here) restated with
+// floating-point expansions (Shewchuk 1997: error-free two-sum and
+// two-product, grow-expansion).  The determinant is the 4x4 one of the rows
+// (x, y, z, 1), i.e. the signed sum of the 24 products x_i y_j z_k over
+// distinct rows i, j, k with the sign of the permutation (i, j, k, l).
+static void expansion_grow(std::vector<double> &e, double b) {
+  std::vector<double> h;
+  double q = b;
+  for (double ei : e) {
+    const double s = q + ei;
+    const double bb = s - q;
+    const double err = (q - (s - bb)) + (ei - bb);
+    q = s;
+    if (err != 0.0) h.push_back(err);
+  }
+  if (q != 0.0 || h.empty()) h.push_back(q);
+  e.swap(h);
+}
+
+static int orient3d_exact_sign(const V3 &a, const V3 &b, const V3 &c, const V3 &d) {
+  const V3 *r[4] = {&a, &b, &c, &d};
+  std::vector<double> e;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j)
+      for (int k = 0; k < 4; ++k) {
+        if (i == j || i == k || j == k) continue;
+        const int l = 6 - i - j - k;
+        // parity of the permutation (i, j, k, l) by counting inversions
+        const int p[4] = {i, j, k, l};
+        int inv = 0;
+        for (int u = 0; u < 4; ++u)
+          for (int v = u + 1; v < 4; ++v) inv += p[u] > p[v];
+        const double sg = (inv & 1) ? -1.0 : 1.0;
+        const double x = (*r[i])[0], y = (*r[j])[1], z = (*r[k])[2];
+        const double hi = x * y, lo = std::fma(x, y, -hi);
+        const double t1 = hi * z, t1e = std::fma(hi, z, -t1);
+        const double t2 = lo * z, t2e = std::fma(lo, z, -t2);
+        expansion_grow(e, sg * t2e);
+        expansion_grow(e, sg * t2);
+        expansion_grow(e, sg * t1e);
+        expansion_grow(e, sg * t1);
+      }
+  for (int i = (int)e.size() - 1; i >= 0; --i)
+    if (e[i] != 0.0) return e[i] > 0.0 ? 1 : -1;
+  return 0;
+}
+
+// orient3d(a,b,c,d) = det[a-d; b-d; c-d]: a floating-point filter, then the
+// exact sign
 static double orient3d(const V3 &a, const V3 &b, const V3 &c, const V3 &d) {
   double adx = a[0] - d[0], bdx = b[0] - d[0], cdx = c[0] - d[0];
   double ady = a[1] - d[1], bdy = b[1] - d[1], cdy = c[1] - d[1];
@@ -180,12 +228,7 @@ static double orient3d(const V3 &a, const V3 &b, const V3 &c, const V3 &d) {
                 (std::fabs(cdy * adz) + std::fabs(cdz * ady)) * std::fabs(bdx) +
                 (std::fabs(ady * bdz) + std::fabs(adz * bdy)) * std::fabs(cdx);
   if (std::fabs(det) > 1e-14 * perm) return det;
-  typedef long double LD;
-  LD Adx = (LD)a[0] - d[0], Bdx = (LD)b[0] - d[0], Cdx = (LD)c[0] - d[0];
-  LD Ady = (LD)a[1] - d[1], Bdy = (LD)b[1] - d[1], Cdy = (LD)c[1] - d[1];
-  LD Adz = (LD)a[2] - d[2], Bdz = (LD)b[2] - d[2], Cdz = (LD)c[2] - d[2];
-  LD D = Adx * (Bdy * Cdz - Bdz * Cdy) + Bdx * (Cdy * Adz - Cdz * Ady) + Cdx * (Ady * Bdz - Adz * Bdy);
-  return (double)D;
+  return (double)orient3d_exact_sign(a, b, c, d);
 }
 
 // em_mesh.h:208-230
