@@ -24,6 +24,9 @@ cpu_baseline : the CPU oracle (restatement of the reference path) on a bounded
          sample of the full-size workload (assembly, AMS setup, one FGMRES
          iteration), extrapolated by the inner iteration count of complete
          oracle solves of it; rank 0, N=1 only
+Under torchrun (N > 1) every rank runs the timed replica steps, the profiled
+step and e2e; plain_fp64, field_err_vs_fp64, dual and warm_start are N=1
+reports and are left out there.
 
 --impl reference times complete CPU-oracle solves (the reference's own
 MPI/PETSc binary cannot be built in this image), one column per step, on the
@@ -671,14 +674,17 @@ def ours(args):
 
     # ---- learned warm start: anchors, training, predicted remainder ---------
     warm = None
-    if not args.no_warm and freqs.size >= 3:
+    # the side arms (warm start, dual, plain FP64, accuracy) are N=1 reports;
+    # under torchrun every rank would repeat them, so N>1 runs skip them
+    single = world == 1
+    if single and not args.no_warm and freqs.size >= 3:
         warm = warm_start_arm(args, ctx, cols, rhs, ne, infos_headline)
 
     rx = np.asarray(prob.survey.rx, dtype=np.float64)
     rx_tets = ctx.find_cell_around_point(rx)
     # ---- dual solves (rtol 1e-6), timed separately ----------------------------
     dual = None
-    if not args.no_dual and (rx_tets >= 0).all():
+    if single and not args.no_dual and (rx_tets >= 0).all():
         log("dual solves")
         kd = freqs.size
         d = torch.zeros((ne, kd), dtype=torch.complex128, device="cuda")
@@ -757,7 +763,7 @@ def ours(args):
     plain = None
     plain_fields = {}
     log("plain FP64 path")
-    if args.plain_freqs != 0:
+    if single and args.plain_freqs != 0:
         npf = freqs.size if args.plain_freqs < 0 else min(args.plain_freqs, freqs.size)
         idx = np.unique(np.linspace(0, freqs.size - 1, npf).round().astype(int))
         # CSEM sweeps: at most --plain-tx transmitters per frequency
@@ -805,7 +811,7 @@ def ours(args):
 
     # ---- accuracy of the headline solution against an FP64 solve ------------
     accuracy = None
-    if not args.no_accuracy and (rx_tets >= 0).all():
+    if single and not args.no_accuracy and (rx_tets >= 0).all():
         log("FP64 reference solve")
         x64 = torch.zeros_like(x)
         inf64 = ctx.solve_block_dev(colf, rhs.data_ptr(), x64.data_ptr(), rtol=1e-12, max_it=800,
